@@ -1,0 +1,277 @@
+"""ctypes binding of the C ABI (include/xsec_b200.h) for tests and bench.py.
+
+The library is built in-tree by gpu_cross_b200.build; loading fails loudly
+when it is missing -- there is no CPU fallback anywhere in this package.
+Device buffers are torch CUDA tensors passed by data pointer.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+from . import build as _build
+
+XS_OK = 0
+XS_ERR_INVALID, XS_ERR_CUDA, XS_ERR_NOMEM, XS_ERR_UNSORTED, XS_ERR_GRID = 1, 2, 3, 4, 5
+XS_ERR_STATE, XS_ERR_NODEVICE, XS_ERR_TIMEOUT, XS_ERR_UNSUPPORTED = 6, 7, 8, 9
+
+GAUSSIAN, DOPPLER, VOIGT, PSUEDO_VOIGT = 0, 1, 2, 3
+CONV_GPU, CONV_CPU = 0, 1
+FP64, MIXED = 0, 1
+
+
+class XsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"xsec_b200 error {code}: {msg}")
+        self.code = code
+
+
+class CrossSectionData(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in
+                ("halfwidth", "mean_mass", "temperature", "pressure", "beta", "partition", "ln2",
+                 "ref_temp", "cmcoef", "dfreq")]
+
+
+class Condition(ctypes.Structure):
+    _fields_ = [("temperature", ctypes.c_double), ("partition", ctypes.c_double),
+                ("pressure", ctypes.c_double), ("gamma_scale", ctypes.c_double),
+                ("cut", ctypes.c_double)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("profile", ctypes.c_int), ("convention", ctypes.c_int),
+                ("precision", ctypes.c_int), ("cpu_threads", ctypes.c_int),
+                ("mean_mass", ctypes.c_double), ("ref_temp", ctypes.c_double),
+                ("half_width", ctypes.c_double), ("dfreq", ctypes.c_double),
+                ("points_per_thread", ctypes.c_int), ("warps_per_block", ctypes.c_int)]
+
+
+class Lines(ctypes.Structure):
+    _fields_ = [("nu", ctypes.c_void_p), ("energies", ctypes.c_void_p), ("aif", ctypes.c_void_p),
+                ("gns", ctypes.c_void_p), ("gamma", ctypes.c_void_p), ("n", ctypes.c_void_p),
+                ("count", ctypes.c_size_t)]
+
+
+class GridC(ctypes.Structure):
+    _fields_ = [("freq", ctypes.c_void_p), ("npoints_total", ctypes.c_int),
+                ("start_idx", ctypes.c_int), ("points", ctypes.c_int)]
+
+
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_SZ = ctypes.c_size_t
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "xs_last_error": (ctypes.c_char_p, []),
+    "xs_version": (ctypes.c_char_p, []),
+    "xs_device_available": (_I, []),
+    "xs_copy_intensity_info": (_I, [ctypes.POINTER(CrossSectionData)]),
+    "xs_execute_two_step_kernal_voigt_block": (_I, [_VP] * 8 + [_I, _I, _I]),
+    "xs_execute_two_step_kernal_doppler_block": (_I, [_VP] * 6 + [_I, _I, _I]),
+    "xs_execute_two_step_kernal_block": (_I, [_VP] * 6 + [_I, _I, _I]),
+    "xs_launcher_sync": (_I, []),
+    "xs_engine_create": (_I, [_I, ctypes.POINTER(_VP)]),
+    "xs_engine_destroy": (_I, [_VP]),
+    "xs_engine_set_stream": (_I, [_VP, _VP]),
+    "xs_engine_sync": (_I, [_VP]),
+    "xs_engine_scratch_bytes": (_I, [_VP, ctypes.POINTER(_SZ)]),
+    "xs_scratch_bytes_needed": (_SZ, [ctypes.POINTER(Options), _I, _SZ]),
+    "xs_engine_execute": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _I,
+                               ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _SZ]),
+    "xs_engine_last_stats": (_I, [_VP, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "xs_manager_create": (_I, [_I, _I, _I, _I, _SZ, ctypes.POINTER(_VP)]),
+    "xs_manager_destroy": (_I, [_VP]),
+    "xs_manager_set_precision": (_I, [_VP, _I]),
+    "xs_manager_initialize_vectors": (_I, [_VP, _I]),
+    "xs_manager_initialize_constants": (_I, [_VP] + [_D] * 7),
+    "xs_manager_transfer_vectors": (_I, [_VP, _SZ] + [_VP] * 6),
+    "xs_manager_transfer_freq": (_I, [_VP, _VP, _VP, _I]),
+    "xs_manager_execute_cross_section": (_I, [_VP, _I, _I, _I]),
+    "xs_manager_transfer_results": (_I, [_VP, _VP, _VP, _I]),
+    "xs_manager_cleanup": (_I, [_VP]),
+    "xs_manager_ready_for_work": (_I, [_VP, ctypes.POINTER(_I)]),
+    "xs_manager_get_ntrans": (_I, [_VP, ctypes.POINTER(_SZ)]),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def library_path() -> str:
+    return _build.LIB_CUDA
+
+
+def declared_functions() -> list[str]:
+    """Function names declared in include/xsec_b200.h."""
+    hdr = os.path.join(_build.INCLUDE, "xsec_b200.h")
+    text = open(hdr).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(xs_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        path = library_path()
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is not built; run python -m gpu_cross_b200.build "
+                              "(there is no CPU fallback)")
+        L = ctypes.CDLL(path)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != XS_OK:
+        msg = lib().xs_last_error()
+        raise XsError(rc, msg.decode() if msg else "")
+
+
+def device_available() -> bool:
+    return bool(lib().xs_device_available())
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    return int(t.data_ptr())
+
+
+class Engine:
+    """One engine handle (device scratch, stream, timing events)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().xs_engine_create(device, ctypes.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self.h:
+            lib().xs_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        check(lib().xs_engine_set_stream(self.h, stream_handle))
+
+    def sync(self) -> None:
+        check(lib().xs_engine_sync(self.h))
+
+    def scratch_bytes(self) -> int:
+        v = ctypes.c_size_t()
+        check(lib().xs_engine_scratch_bytes(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def execute(self, opts: Options, conds: list[Condition], lines: Lines, grid: GridC, out_ptr: int,
+                out_stride: int = 0) -> None:
+        arr = (Condition * len(conds))(*conds)
+        check(lib().xs_engine_execute(self.h, ctypes.byref(opts), arr, len(conds),
+                                      ctypes.byref(lines), ctypes.byref(grid), out_ptr, out_stride))
+
+    def last_stats(self) -> tuple[float, float]:
+        a, b = ctypes.c_double(), ctypes.c_double()
+        check(lib().xs_engine_last_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return float(a.value), float(b.value)
+
+
+def make_lines(dev: dict, count: int | None = None) -> Lines:
+    """dev: dict of torch CUDA tensors nu, energies, aif, gns, gamma, n."""
+    n = int(dev["nu"].numel()) if count is None else count
+    return Lines(_ptr(dev["nu"]), _ptr(dev["energies"]), _ptr(dev["aif"]), _ptr(dev["gns"]),
+                 _ptr(dev.get("gamma")), _ptr(dev.get("n")), n)
+
+
+def make_grid(freq, start_idx: int = 0, points: int | None = None) -> GridC:
+    total = int(freq.numel())
+    pts = total - start_idx if points is None else points
+    return GridC(_ptr(freq), total, start_idx, pts)
+
+
+def make_options(profile: int, dfreq: float, mean_mass: float, convention: int = CONV_GPU,
+                 precision: int = FP64, cpu_threads: int = 1, ref_temp: float = 296.0,
+                 half_width: float = 0.1, points_per_thread: int = 0,
+                 warps_per_block: int = 0) -> Options:
+    return Options(profile, convention, precision, cpu_threads, mean_mass, ref_temp, half_width,
+                   dfreq, points_per_thread, warps_per_block)
+
+
+def make_condition(temperature: float, partition: float, pressure: float = 1.0,
+                   gamma_scale: float = 1.0, cut: float = -1.0) -> Condition:
+    return Condition(temperature, partition, pressure, gamma_scale, cut)
+
+
+class Manager:
+    """The BaseManager interface (BaseManager.h:22-30) over host numpy
+    arrays.  kind 0 = GpuManager, 1 = OpenMPManager (computed on the GPU)."""
+
+    def __init__(self, kind: int, profile: int, gpu_id: int = 0, num_threads: int = 1,
+                 total_memory: int = 1_000_000_000):
+        h = ctypes.c_void_p()
+        check(lib().xs_manager_create(kind, profile, gpu_id, num_threads, total_memory,
+                                      ctypes.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().xs_manager_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _np(a):
+        return None if a is None else a.ctypes.data
+
+    def set_precision(self, p: int) -> None:
+        check(lib().xs_manager_set_precision(self.h, p))
+
+    def InitializeVectors(self, npoints: int) -> None:
+        check(lib().xs_manager_initialize_vectors(self.h, npoints))
+
+    def InitializeConstants(self, half_width, temperature, partition, dfreq, meanmass,
+                            pressure=10.0, ref_temp=296.0) -> None:
+        check(lib().xs_manager_initialize_constants(self.h, half_width, temperature, partition,
+                                                    dfreq, meanmass, pressure, ref_temp))
+
+    def TransferVectors(self, nener, energies, nu, aif, gns, gamma=None, n=None) -> None:
+        check(lib().xs_manager_transfer_vectors(self.h, nener, self._np(energies), self._np(nu),
+                                                self._np(aif), self._np(gns), self._np(gamma),
+                                                self._np(n)))
+
+    def TransferFreq(self, freq, intens, n) -> None:
+        check(lib().xs_manager_transfer_freq(self.h, self._np(freq), self._np(intens), n))
+
+    def ExecuteCrossSection(self, n, n_ener, start_idx) -> None:
+        check(lib().xs_manager_execute_cross_section(self.h, n, n_ener, start_idx))
+
+    def TransferResults(self, freq, intens, n) -> None:
+        check(lib().xs_manager_transfer_results(self.h, self._np(freq), self._np(intens), n))
+
+    def Cleanup(self) -> None:
+        check(lib().xs_manager_cleanup(self.h))
+
+    def ReadyForWork(self) -> bool:
+        v = ctypes.c_int()
+        check(lib().xs_manager_ready_for_work(self.h, ctypes.byref(v)))
+        return bool(v.value)
+
+    def GetNtrans(self) -> int:
+        v = ctypes.c_size_t()
+        check(lib().xs_manager_get_ntrans(self.h, ctypes.byref(v)))
+        return int(v.value)

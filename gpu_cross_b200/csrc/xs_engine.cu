@@ -1,0 +1,444 @@
+// Host side of the engine and the C ABI declared in include/xsec_b200.h.
+//
+// An engine owns a stream, a grow-only device scratch area (per-line records
+// and windows for every condition of a call) and two device words (an error
+// word the kernels OR bits into, and the work counter of the persistent step
+// two).  xs_engine_execute computes the per-condition constants on the host
+// exactly as the chosen reference backend does, then launches
+//   grid check -> step one (k_prep) -> step two (persistent warps)
+// on the engine's stream.  Nothing is synchronised until xs_engine_sync,
+// which also turns the error word into a status code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "xs_engine.h"
+#include "xs_internal.cuh"
+#include "xsec_b200.h"
+
+using namespace xs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? XS_ERR_NOMEM : XS_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define XS_CU(call)                                     \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+struct xs_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    void* scratch = nullptr;
+    size_t scratch_cap = 0;
+    unsigned* d_words = nullptr;  // [0] error bits, [1] work counter
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    bool timed = false;
+    std::mutex mu;
+};
+
+namespace xs {
+
+int set_error(int code, const char* msg) { return fail(code, msg); }
+
+// Default launch shapes (tuned on a B200; the autotuner may override them).
+void default_shape(int kind, bool mixed, int* P, int* warps) {
+    if (kind == kVoigt) {
+        *P = mixed ? 4 : 2;
+        *warps = 8;
+    } else {
+        *P = 1;
+        *warps = 8;
+    }
+}
+
+// Host copy of the per-condition constants.  GPU convention:
+// GpuManager::InitializeConstants (GPUManager.cpp:28-39) and the step-two
+// kernels (cross_kernal.cu:667, :938-939).  CPU convention: OpenMPManager
+// (OpenMPManager.cpp:65-66, :146-147, :191-192).
+CondDev make_cond(const xs_options& o, const xs_condition& c) {
+    CondDev d{};
+    const double T = c.temperature;
+    const double M = o.mean_mass;
+    if (o.convention == XS_CONV_GPU) {
+        const double planck = 6.6260693e-27, vellgt = 2.99792458e10, boltz = 1.380658e-16;
+        const double pi = std::acos(-1.0);
+        d.cmcoef = 1.0 / (8.0 * pi * vellgt);
+        d.beta = planck * vellgt / (boltz * T);
+        d.dpw = std::sqrt(2.0 * kBOLTZ * T * kNA / (M)) / kVELLGT;
+    } else {
+        d.cmcoef = 1.0 / (8.0 * kPI * kVELLGT);
+        d.beta = kPLANCK * kVELLGT / (kBOLTZ * T);
+        d.dpw = std::sqrt(2.0 * kLN2 * kBOLTZ * T * kNA / (M)) / kVELLGT;
+    }
+    d.partition = c.partition;
+    d.tratio = o.ref_temp / T;
+    d.gamma_scale = c.gamma_scale > 0.0 ? c.gamma_scale : 1.0;
+    if (c.cut > 0.0) {
+        d.cut = c.cut;
+    } else if (o.profile == XS_VOIGT) {
+        d.cut = std::fmin(25.0 * c.pressure, 100.0);
+    } else if (o.profile == XS_DOPPLER) {
+        d.cut = kDOPPLER_CUTOFF;
+    } else {
+        d.cut = o.half_width * 10.0;
+    }
+    return d;
+}
+
+// Lines the CPU convention covers: OpenMPManager splits N lines into blocks
+// of ceil(float(N)/float(threads)) (OpenMPManager.cpp:186-188); lines beyond
+// threads * block are never processed.
+long cpu_covered_lines(long n, int threads) {
+    if (threads < 1) return n;
+    const int nener = int(n);
+    const int for_block = int(std::ceil(float(nener) / float(threads)));
+    const long covered = long(threads) * long(for_block);
+    return covered < n ? covered : n;
+}
+
+}  // namespace xs
+
+extern "C" {
+
+const char* xs_last_error(void) { return g_last_error.c_str(); }
+
+const char* xs_version(void) { return "xsec_b200 0.1 (sm_100a)"; }
+
+int xs_device_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    for (int d = 0; d < n; ++d) {
+        int major = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) == cudaSuccess &&
+            major == 10)
+            return 1;
+    }
+    return 0;
+}
+
+int xs_engine_create(int device, xs_engine** out) {
+    if (!out) return fail(XS_ERR_INVALID, "xs_engine_create: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return fail(XS_ERR_NODEVICE, "xs_engine_create: no such CUDA device");
+    }
+    int major = 0;
+    XS_CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major != 10)
+        return fail(XS_ERR_NODEVICE, "xs_engine_create: the kernels are built for sm_100a only");
+    DeviceGuard g(device);
+    auto* e = new xs_engine();
+    e->device = device;
+    XS_CU(cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, device));
+    cudaError_t err = cudaMalloc(&e->d_words, 4 * sizeof(unsigned));
+    if (err != cudaSuccess) {
+        delete e;
+        return cuda_fail(err, "cudaMalloc(engine words)");
+    }
+    err = cudaMemset(e->d_words, 0, 4 * sizeof(unsigned));
+    for (auto& ev : e->ev)
+        if (err == cudaSuccess) err = cudaEventCreate(&ev);
+    if (err != cudaSuccess) {
+        xs_engine_destroy(e);
+        return cuda_fail(err, "xs_engine_create");
+    }
+    *out = e;
+    return XS_OK;
+}
+
+int xs_engine_destroy(xs_engine* e) {
+    if (!e) return XS_OK;
+    {
+        DeviceGuard g(e->device);
+        if (e->stream) cudaStreamSynchronize(e->stream);
+        else cudaDeviceSynchronize();
+        for (auto& ev : e->ev)
+            if (ev) cudaEventDestroy(ev);
+        cudaFree(e->scratch);
+        cudaFree(e->d_words);
+    }
+    delete e;
+    return XS_OK;
+}
+
+int xs_engine_set_stream(xs_engine* e, void* stream) {
+    if (!e) return fail(XS_ERR_INVALID, "xs_engine_set_stream: NULL engine");
+    std::lock_guard<std::mutex> lk(e->mu);
+    e->stream = static_cast<cudaStream_t>(stream);
+    return XS_OK;
+}
+
+int xs_engine_sync(xs_engine* e) {
+    if (!e) return fail(XS_ERR_INVALID, "xs_engine_sync: NULL engine");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    XS_CU(cudaStreamSynchronize(e->stream));
+    unsigned w = 0;
+    XS_CU(cudaMemcpy(&w, e->d_words, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (w) {
+        XS_CU(cudaMemset(e->d_words, 0, sizeof(unsigned)));
+        if (w & kErrUnsorted)
+            return fail(XS_ERR_UNSORTED, "line centres are not in ascending order (the reference "
+                                         "requires nu-sorted input)");
+        if (w & kErrGrid)
+            return fail(XS_ERR_GRID, "the grid is not ascending with the uniform step dfreq");
+    }
+    return XS_OK;
+}
+
+int xs_engine_scratch_bytes(xs_engine* e, size_t* bytes) {
+    if (!e || !bytes) return fail(XS_ERR_INVALID, "xs_engine_scratch_bytes: NULL argument");
+    *bytes = e->scratch_cap;
+    return XS_OK;
+}
+
+size_t xs_scratch_bytes_needed(const xs_options* opt, int ncond, size_t n_lines) {
+    if (!opt || ncond < 1) return 0;
+    const bool mixed = opt->profile == XS_VOIGT && opt->precision == XS_MIXED;
+    const size_t per = record_bytes(opt->profile, mixed) + aux_bytes(opt->profile, mixed) + 2 * sizeof(int);
+    const int nc = ncond < kMaxCond ? ncond : kMaxCond;
+    return align_up(per * n_lines * size_t(nc) + 4 * 256, 256);
+}
+
+int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                      const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride) {
+    return xs::engine_execute(e, opt, conds, ncond, lines, grid, out, out_stride, nullptr);
+}
+
+int xs_engine_last_stats(xs_engine* e, double* prep_ms, double* steptwo_ms) {
+    if (!e) return fail(XS_ERR_INVALID, "xs_engine_last_stats: NULL engine");
+    if (!e->timed) return fail(XS_ERR_STATE, "xs_engine_last_stats: nothing executed yet");
+    DeviceGuard g(e->device);
+    XS_CU(cudaEventSynchronize(e->ev[2]));
+    float a = 0.f, b = 0.f;
+    XS_CU(cudaEventElapsedTime(&a, e->ev[0], e->ev[1]));
+    XS_CU(cudaEventElapsedTime(&b, e->ev[1], e->ev[2]));
+    if (prep_ms) *prep_ms = a;
+    if (steptwo_ms) *steptwo_ms = b;
+    return XS_OK;
+}
+
+}  // extern "C"
+
+namespace xs {
+
+int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                   const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride,
+                   const ExecOverride* ov) {
+    if (!e || !opt || !conds || !lines || !grid || !out)
+        return fail(XS_ERR_INVALID, "xs_engine_execute: NULL argument");
+    const int kind = opt->profile;
+    if (kind == XS_PSUEDO_VOIGT)
+        return fail(XS_ERR_UNSUPPORTED, "PSUEDO_VOIGT is not implemented (nor is it in the reference)");
+    if (kind != XS_VOIGT && kind != XS_DOPPLER && kind != XS_GAUSSIAN)
+        return fail(XS_ERR_INVALID, "unknown profile");
+    if (opt->convention != XS_CONV_GPU && opt->convention != XS_CONV_CPU)
+        return fail(XS_ERR_INVALID, "unknown convention");
+    if (kind == XS_GAUSSIAN && opt->convention == XS_CONV_CPU)
+        return fail(XS_ERR_UNSUPPORTED, "the reference CPU backend has no GAUSSIAN profile");
+    if (opt->precision != XS_FP64 && opt->precision != XS_MIXED)
+        return fail(XS_ERR_INVALID, "unknown precision");
+    if (ncond < 1) return fail(XS_ERR_INVALID, "ncond < 1");
+    if (!(opt->dfreq > 0.0)) return fail(XS_ERR_INVALID, "dfreq must be > 0");
+    if (!(opt->mean_mass > 0.0) && kind != XS_GAUSSIAN)
+        return fail(XS_ERR_INVALID, "mean_mass must be > 0");
+    if (kind == XS_GAUSSIAN && !(opt->half_width > 0.0))
+        return fail(XS_ERR_INVALID, "half_width must be > 0 for GAUSSIAN");
+    if (!grid->freq || grid->npoints_total < 1 || grid->start_idx < 0 || grid->points < 0 ||
+        long(grid->start_idx) + long(grid->points) > long(grid->npoints_total))
+        return fail(XS_ERR_INVALID, "grid chunk outside the grid");
+    if (ncond > 1 && out_stride < size_t(grid->npoints_total))
+        return fail(XS_ERR_INVALID, "out_stride smaller than the grid");
+    if (lines->count > 0 && (!lines->nu || !lines->energies || !lines->aif || !lines->gns))
+        return fail(XS_ERR_INVALID, "line arrays missing");
+    if (kind == XS_VOIGT && lines->count > 0 && (!lines->gamma || !lines->n))
+        return fail(XS_ERR_INVALID, "VOIGT needs gamma and n");
+    if (lines->count > size_t(INT32_MAX))
+        return fail(XS_ERR_INVALID, "more than 2^31-1 lines in one call");
+    for (int c = 0; c < ncond; ++c)
+        if (!(conds[c].temperature > 0.0))
+            return fail(XS_ERR_INVALID, "temperature must be > 0");
+    const bool mixed = kind == XS_VOIGT && opt->precision == XS_MIXED;
+    if (mixed && double(grid->npoints_total) > 15.0e6)
+        return fail(XS_ERR_UNSUPPORTED, "mixed precision supports grids below 1.5e7 points");
+
+    long n = long(lines->count);
+    if (opt->convention == XS_CONV_CPU) n = cpu_covered_lines(n, opt->cpu_threads);
+    if (n <= 0 || grid->points <= 0) return XS_OK;
+
+    int P = opt->points_per_thread, W = opt->warps_per_block;
+    {
+        int dP, dW;
+        default_shape(kind, mixed, &dP, &dW);
+        if (P == 0) P = dP;
+        if (W == 0) W = dW;
+    }
+    if (kind == XS_VOIGT ? !(P == 1 || P == 2 || P == 4 || P == 8) : !(P == 1 || P == 2))
+        return fail(XS_ERR_INVALID, "points_per_thread must be 1, 2, 4 or 8 (1 or 2 for erf profiles)");
+    if (W != 4 && W != 8) return fail(XS_ERR_INVALID, "warps_per_block must be 4 or 8");
+
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard dg(e->device);
+
+    // Scratch layout for one group of conditions.
+    const size_t rb = record_bytes(kind, mixed), ab = aux_bytes(kind, mixed);
+    const int group = ncond < kMaxCond ? ncond : kMaxCond;
+    const size_t nl = size_t(n);
+    const size_t off_rec = 0;
+    const size_t off_aux = align_up(off_rec + rb * nl * group, 256);
+    const size_t off_wlo = align_up(off_aux + ab * nl * group, 256);
+    const size_t off_whi = align_up(off_wlo + sizeof(int) * nl * group, 256);
+    const size_t need = align_up(off_whi + sizeof(int) * nl * group, 256);
+
+    void* scratch = nullptr;
+    unsigned* words = e->d_words;
+    if (ov && ov->scratch) {
+        if (need > ov->scratch_bytes)
+            return fail(XS_ERR_NOMEM, "scratch larger than the caller-provided area");
+        scratch = ov->scratch;
+        if (ov->words) words = ov->words;
+    } else {
+        if (need > e->scratch_cap) {
+            XS_CU(cudaStreamSynchronize(e->stream));
+            cudaFree(e->scratch);
+            e->scratch = nullptr;
+            e->scratch_cap = 0;
+            cudaError_t err = cudaMalloc(&e->scratch, need);
+            if (err != cudaSuccess) {
+                cudaGetLastError();
+                return cuda_fail(err, "cudaMalloc(scratch)");
+            }
+            e->scratch_cap = need;
+        }
+        scratch = e->scratch;
+    }
+    char* base = static_cast<char*>(scratch);
+
+    GridDev G;
+    G.freq = grid->freq;
+    G.f0 = 0.0;  // kernels read freq[0] on the device
+    G.df = opt->dfreq;
+    G.npoints_total = grid->npoints_total;
+    G.start = grid->start_idx;
+    G.points = grid->points;
+
+    LinesDev L;
+    L.nu = lines->nu;
+    L.energies = lines->energies;
+    L.aif = lines->aif;
+    L.gamma = lines->gamma;
+    L.nexp = lines->n;
+    L.gns = lines->gns;
+    L.n = n;
+
+    const cudaStream_t st = e->stream;
+    const bool timing = !(ov && ov->no_timing);
+    cudaError_t err = launch_grid_check(G, words, st);
+    if (err != cudaSuccess) return cuda_fail(err, "grid check launch");
+
+    for (int c0 = 0; c0 < ncond; c0 += group) {
+        const int nc = std::min(group, ncond - c0);
+        PrepArgs pa;
+        std::memset(&pa, 0, sizeof(pa));
+        pa.L = L;
+        pa.G = G;
+        pa.ncond = nc;
+        for (int c = 0; c < nc; ++c) {
+            pa.cond[c] = make_cond(*opt, conds[c0 + c]);
+            if (ov && ov->use_consts) {
+                pa.cond[c].cmcoef = ov->cmcoef;
+                pa.cond[c].beta = ov->beta;
+            }
+        }
+        pa.rec = base + off_rec;
+        pa.aux = ab ? base + off_aux : nullptr;
+        pa.wlo = reinterpret_cast<int*>(base + off_wlo);
+        pa.whi = reinterpret_cast<int*>(base + off_whi);
+        pa.err = words;
+        pa.half_width = opt->half_width;
+        pa.x0 = opt->dfreq * 0.5;
+        if (kind == XS_GAUSSIAN) {
+            pa.xg = std::sqrt(kLN2) / opt->half_width;
+            pa.x0g = pa.xg * opt->dfreq * 0.5;
+        }
+        pa.mixed_tile_span = 32 * P;
+
+        if (timing && c0 == 0) cudaEventRecord(e->ev[0], st);
+        err = launch_prep(kind, opt->convention, mixed, pa, st);
+        if (err != cudaSuccess) return cuda_fail(err, "step one launch");
+        if (timing && c0 == 0) cudaEventRecord(e->ev[1], st);
+
+        StepArgs sa;
+        std::memset(&sa, 0, sizeof(sa));
+        sa.rec = pa.rec;
+        sa.aux = static_cast<const AuxV64*>(pa.aux);
+        sa.wlo = pa.wlo;
+        sa.whi = pa.whi;
+        sa.n = n;
+        sa.out = out + size_t(c0) * out_stride;
+        sa.out_stride = out_stride;
+        sa.G = G;
+        sa.tiles_per_cond = (grid->points + 32 * P - 1) / (32 * P);
+        sa.n_items = sa.tiles_per_cond * nc;
+        sa.counter = words + 1;
+        sa.x0 = pa.x0;
+        sa.xg = pa.xg;
+        sa.x0g = pa.x0g;
+        err = cudaMemsetAsync(sa.counter, 0, sizeof(unsigned), st);
+        if (err != cudaSuccess) return cuda_fail(err, "counter reset");
+        int occ = steptwo_blocks_per_sm(kind, opt->convention, mixed, P, W);
+        if (occ < 1) occ = 1;
+        const long want = (long(sa.n_items) + W - 1) / W;
+        const int blocks = int(std::min<long>(want, long(occ) * e->num_sms));
+        err = launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);
+        if (err != cudaSuccess) return cuda_fail(err, "step two launch");
+        if (timing && c0 + nc >= ncond) {
+            cudaEventRecord(e->ev[2], st);
+            e->timed = true;
+        }
+    }
+    return XS_OK;
+}
+
+}  // namespace xs

@@ -1,0 +1,31 @@
+// Internal engine entry shared by the C ABI files (launcher and manager
+// levels).  Not part of the public ABI.
+#pragma once
+
+#include <cstddef>
+
+#include "xsec_b200.h"
+
+namespace xs {
+
+struct CondDev;
+
+// Optional knobs of one execute call.
+struct ExecOverride {
+    void* scratch = nullptr;      // caller-provided scratch area (device)
+    size_t scratch_bytes = 0;
+    unsigned* words = nullptr;    // caller-provided error word + counter (device)
+    bool no_timing = false;       // skip the CUDA events
+    bool use_consts = false;      // take cmcoef and beta from below instead of
+    double cmcoef = 0.0;          //   recomputing them from T (launcher level:
+    double beta = 0.0;            //   the cross_section_data the caller copied)
+};
+
+int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                   const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride,
+                   const ExecOverride* ov);
+
+int set_error(int code, const char* msg);
+long cpu_covered_lines(long n, int threads);
+
+}  // namespace xs

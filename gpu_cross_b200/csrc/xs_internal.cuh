@@ -1,0 +1,149 @@
+// Internal declarations shared by the kernels (xs_kernels.cu) and the host
+// engine (xs_engine.cu).  Not part of the public C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace xs {
+
+// Physical constants, defines.h:4-20 of the reference (the values must match
+// bit-for-bit; GPUManager.cpp:28-31 uses the same literals).
+constexpr double kLN2 = 0.69314718056;
+constexpr double kISQRTPI = 0.564189584;
+constexpr double kPI = 3.14159265359;
+constexpr double kPLANCK = 6.6260693e-27;
+constexpr double kVELLGT = 2.99792458e+10;
+constexpr double kBOLTZ = 1.380658e-16;
+constexpr double kNA = 6.0221412927e23;
+constexpr double kDOPPLER_CUTOFF = 100.0;
+
+// Region I constant of Humlicek's W4 (T * 0.5641896 / (0.5 + T^2)).
+constexpr double kW4C = 0.5641896;
+
+// |t| at and beyond which erf(t) is exactly +-1 in double precision
+// (erfc(6) = 2.2e-17 < 2^-54); tests/test_gpu_parity.py checks the device erf
+// against it.  Doppler/Gaussian pairs whose both erf arguments lie beyond it
+// add exactly 0 in the reference and are skipped.
+constexpr double kErfSat = 6.0;
+
+enum Kind : int { kGauss = 0, kDoppler = 1, kVoigt = 2 };
+enum Conv : int { kConvGpu = 0, kConvCpu = 1 };
+
+// Device-side error bits (OR-ed into the engine's error word).
+constexpr unsigned kErrUnsorted = 1u;
+constexpr unsigned kErrGrid = 2u;
+
+constexpr int kMaxCond = 64;  // conditions per launch (the sweep uses 40)
+
+// Per-condition constants, computed on the host exactly as the selected
+// reference backend computes them (GPUManager.cpp:24-47 for the GPU
+// convention, OpenMPManager.cpp:57-67 and :146-147/:191-192 for the CPU one).
+struct CondDev {
+    double cmcoef;       // 1/(8 pi c)
+    double beta;         // hc/kT
+    double partition;    // Q(T)
+    double tratio;       // ref_temp / T (base of the gamma temperature power)
+    double dpw;          // Doppler width per unit wavenumber
+    double cut;          // window half width (cm-1)
+    double gamma_scale;  // multiplies the uploaded gamma
+    double pad;
+};
+
+// Voigt FP64 record, one per (line, condition).  Region I of W4 written as
+// a real rational in x^2: Re w * pref = (Pc x^2 + Qc) / (x^2 (x^2 + B) + A2)
+// with Pc = pref c y, Qc = Pc (0.5 + y^2), B = 2 y^2 - 1, A2 = (0.5 + y^2)^2.
+struct __align__(16) RecV64 {
+    double nu;   // line centre used for offsets
+    double g;    // 1 / Doppler width
+    double B, A2, Pc, Qc;
+    int lo, hi;    // window [lo, hi) of grid indices
+    int clo, chi;  // grid indices near the core (region I not guaranteed)
+};
+static_assert(sizeof(RecV64) == 64, "RecV64 layout");
+
+// FP64 data for the exact (slow) path of a Voigt pair.
+struct __align__(16) AuxV64 {
+    double nu, g, y, pref;  // pref = S * g
+};
+static_assert(sizeof(AuxV64) == 32, "AuxV64 layout");
+
+// Voigt mixed-precision record (FP32).  The offset of grid point j from the
+// line centre is (m - j) * df + r in cm-1, with m the nearest grid index and
+// |r| <= df/2 computed in FP64; stored scaled by g: x = (m - j) * dfa + ra.
+struct __align__(16) RecV32 {
+    float m, ra, dfa, B;
+    float A2, Pc, Qc, y;
+    float lo, hi, clo, chi;
+};
+static_assert(sizeof(RecV32) == 48, "RecV32 layout");
+
+// Doppler / Gaussian record (FP64).
+struct __align__(16) RecE64 {
+    double nu;  // centre used for offsets
+    double s;   // intensity
+    double g;   // Doppler: 1 / (nu * dpw); Gaussian: unused
+    double pad;
+    int lo, hi;  // active window (reference window, minus pairs that add exactly 0)
+    int pad0, pad1;
+};
+static_assert(sizeof(RecE64) == 48, "RecE64 layout");
+
+struct GridDev {
+    const double* freq;  // full grid
+    double f0, df;       // analytic grid f_j ~ f0 + j * df (f0 = freq[0])
+    int npoints_total;
+    int start, points;   // chunk [start, start + points)
+};
+
+struct LinesDev {
+    const double *nu, *energies, *aif, *gamma, *nexp;
+    const int* gns;
+    long n;  // lines evaluated (may be less than uploaded: CPU coverage rule)
+};
+
+struct PrepArgs {
+    LinesDev L;
+    GridDev G;
+    int ncond;
+    CondDev cond[kMaxCond];
+    void* rec;          // records, condition-major: rec + c * n
+    void* aux;          // AuxV64 (Voigt only)
+    int* wlo;           // windows, condition-major
+    int* whi;
+    unsigned* err;
+    double half_width;  // Gaussian
+    double x0;          // Doppler half bin: dfreq * 0.5
+    double xg, x0g;     // Gaussian: sqrt(ln2)/HW, xg * dfreq * 0.5
+    int mixed_tile_span;  // 32 * points_per_thread (mixed safety bound)
+};
+
+struct StepArgs {
+    const void* rec;
+    const AuxV64* aux;
+    const int* wlo;
+    const int* whi;
+    long n;             // lines per condition
+    double* out;
+    size_t out_stride;  // elements between conditions
+    GridDev G;
+    int tiles_per_cond;
+    int n_items;
+    unsigned* counter;
+    double x0, xg, x0g;  // Doppler / Gaussian constants
+};
+
+// Kernel launchers (xs_kernels.cu).  All asynchronous on `stream`.
+cudaError_t launch_grid_check(const GridDev& g, unsigned* err, cudaStream_t stream);
+cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaStream_t stream);
+// P = points per thread (1, 2, 4, 8), warps per block (4 or 8).
+cudaError_t launch_steptwo(int kind, int conv, bool mixed, int P, int warps, int blocks,
+                           const StepArgs& a, cudaStream_t stream);
+// Resident blocks per SM for a step-two configuration.
+int steptwo_blocks_per_sm(int kind, int conv, bool mixed, int P, int warps);
+size_t record_bytes(int kind, bool mixed);
+size_t aux_bytes(int kind, bool mixed);
+
+}  // namespace xs

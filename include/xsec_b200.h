@@ -1,0 +1,209 @@
+/*
+ * xsec_b200 -- C ABI of the B200 cross-section engine.
+ *
+ * sigma(f_j) = sum_i S_i(T) * Phi_i(f_j - nu_i; T, P) over |f_j - nu_i| <= cut,
+ * for Doppler, Gaussian and Voigt (Humlicek W4) line profiles on a uniform
+ * wavenumber grid, computed by hand-written sm_100a kernels.
+ *
+ * Three levels, all plain C (pointers, sizes, int status codes; no C++ or
+ * torch types):
+ *
+ *  1. Launcher level -- drop-in replacements for the reference's host
+ *     launchers in cross_kernal.cuh (device pointers, default stream,
+ *     constants set once per device).
+ *  2. Engine level -- explicit handle, stream, profile, Doppler-width
+ *     convention, precision (FP64 or mixed FP32/FP64) and batches of (T, P)
+ *     conditions over one resident line list.
+ *  3. Manager level -- the reference's BaseManager interface
+ *     (BaseManager.h:22-30) over host buffers; the C++ classes in
+ *     include/xsec/ (GpuManager, OpenMPManager, ...) sit on these calls.
+ *
+ * Every call returns XS_OK (0) or an XS_ERR_* code; xs_last_error() gives a
+ * message for the calling thread.  Nothing here falls back to the CPU: a
+ * machine without a usable sm_100 device gets XS_ERR_CUDA / XS_ERR_NODEVICE.
+ */
+#ifndef XSEC_B200_H
+#define XSEC_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define XS_OK 0
+#define XS_ERR_INVALID 1   /* bad argument or size */
+#define XS_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define XS_ERR_NOMEM 3     /* device allocation failed / over budget */
+#define XS_ERR_UNSORTED 4  /* line centres not ascending (the reference requires it) */
+#define XS_ERR_GRID 5      /* grid not ascending or not uniform */
+#define XS_ERR_STATE 6     /* call out of order (e.g. execute before upload) */
+#define XS_ERR_NODEVICE 7  /* no usable sm_100 device */
+#define XS_ERR_TIMEOUT 8   /* a bounded device-side wait ran out */
+#define XS_ERR_UNSUPPORTED 9
+
+/* ---- enums -------------------------------------------------------------- */
+/* ProfileType, Input.h:9-15 (same order and values). */
+#define XS_GAUSSIAN 0
+#define XS_DOPPLER 1
+#define XS_VOIGT 2
+#define XS_PSUEDO_VOIGT 3
+
+/* Which reference backend's arithmetic to reproduce.
+ * XS_CONV_GPU: cross_kernal.cu -- Doppler width sqrt(2kT N_A/M)/c, window
+ *   -cut <= nu - f <= cut, cut = min(25 P, 100) (Voigt) or 100 (Doppler).
+ * XS_CONV_CPU: OpenMPManager.cpp -- width with an extra sqrt(ln 2), window
+ *   [round((nu-cut-f0)/df), round((nu+cut-f0)/df)) clamped to the chunk. */
+#define XS_CONV_GPU 0
+#define XS_CONV_CPU 1
+
+/* XS_FP64: every operation in double (matches the reference to <= 1e-10).
+ * XS_MIXED: Voigt profile evaluation and accumulation in FP32 (compensated
+ * per tile), line-centre offsets, intensities and the final per-tile sum in
+ * FP64; Doppler and Gaussian stay FP64. */
+#define XS_FP64 0
+#define XS_MIXED 1
+
+/* cross_section_data, cross_structs.cuh:3-17 (same fields, same order). */
+typedef struct {
+    double halfwidth;
+    double mean_mass;
+    double temperature;
+    double pressure;
+    double beta;
+    double partition;
+    double ln2;
+    double ref_temp;
+    double cmcoef;
+    double dfreq;
+} xs_cross_section_data;
+
+/* One (T, P) condition of a run or sweep. */
+typedef struct {
+    double temperature;  /* K */
+    double partition;    /* Q(T) */
+    double pressure;     /* atm; sets the reference Voigt cut min(25 P, 100) */
+    double gamma_scale;  /* multiplies the uploaded gamma (1.0 when gamma is
+                            already pressure-scaled, as the readers do) */
+    double cut;          /* > 0: window half width in cm-1; <= 0: reference rule */
+} xs_condition;
+
+/* Run options shared by all conditions of one call. */
+typedef struct {
+    int profile;      /* XS_DOPPLER / XS_VOIGT / XS_GAUSSIAN */
+    int convention;   /* XS_CONV_GPU / XS_CONV_CPU */
+    int precision;    /* XS_FP64 / XS_MIXED */
+    int cpu_threads;  /* XS_CONV_CPU only: the OpenMPManager thread count; it
+                         decides which lines the reference covers (blocks of
+                         ceil(float(N)/float(threads)), OpenMPManager.cpp:186) */
+    double mean_mass; /* amu */
+    double ref_temp;  /* K, gamma(T) = gamma * (ref_temp / T)^n */
+    double half_width;/* GAUSSIAN HWHM */
+    double dfreq;     /* grid step (the reference's cross_constants.dfreq) */
+    int points_per_thread; /* 0 = autotuned; else 1, 2, 4 or 8 */
+    int warps_per_block;   /* 0 = autotuned; else 4 or 8 */
+} xs_options;
+
+/* Device-resident line list (structure of arrays, ascending nu). */
+typedef struct {
+    const double* nu;
+    const double* energies; /* lower-state energy E'' (cm-1) */
+    const double* aif;      /* Einstein A (s-1) */
+    const int* gns;         /* upper-state degeneracy */
+    const double* gamma;    /* Lorentz HWHM (cm-1); may be NULL unless VOIGT */
+    const double* n;        /* temperature exponent; may be NULL unless VOIGT */
+    size_t count;
+} xs_lines;
+
+/* Device grid: the reference's f_j = f0 + j*df array (BaseProfile.cpp:19). */
+typedef struct {
+    const double* freq;     /* npoints_total values, ascending, uniform step dfreq */
+    int npoints_total;
+    int start_idx;          /* first point of the chunk evaluated */
+    int points;             /* points in the chunk */
+} xs_grid;
+
+typedef struct xs_engine xs_engine;
+
+/* ---- general ------------------------------------------------------------ */
+const char* xs_last_error(void);
+const char* xs_version(void);
+/* 1 if a usable sm_100 device is present (no context is created otherwise). */
+int xs_device_available(void);
+
+/* ---- 1. launcher level: drop-in for cross_kernal.cuh -------------------- */
+/* copy_intensity_info (cross_kernal.cuh:18): per-device constants used by the
+ * launchers below (current device). */
+int xs_copy_intensity_info(const xs_cross_section_data* cross_inf);
+/* execute_two_step_kernal_voigt_block with gamma (cross_kernal.cuh:45):
+ * g_intens[start_idx .. start_idx+Npoints) += Voigt sum over the first N_ener
+ * lines, reference GPU convention, FP64, legacy default stream, asynchronous.
+ * Unlike the reference, g_energies and g_gamma are not overwritten. */
+int xs_execute_two_step_kernal_voigt_block(double* g_freq, double* g_intens, double* g_energies,
+                                           double* g_nu, int* g_gns, double* g_aif,
+                                           double* g_gamma, double* g_n, int Npoints, int N_ener,
+                                           int start_idx);
+/* execute_two_step_kernal_doppler_block (cross_kernal.cuh:52). */
+int xs_execute_two_step_kernal_doppler_block(double* g_freq, double* g_intens,
+                                             double* g_energies, double* g_nu, int* g_gns,
+                                             double* g_aif, int Npoints, int N_ener,
+                                             int start_idx);
+/* execute_two_step_kernal_block (cross_kernal.cuh:35), GAUSSIAN with
+ * ln2 = 0.69314718056 and the window |f - nu| <= 10 * halfwidth. */
+int xs_execute_two_step_kernal_block(double* g_freq, double* g_intens, double* g_energies,
+                                     double* g_nu, int* g_gns, double* g_aif, int Npoints,
+                                     int N_ener, int start_idx);
+/* Waits for the launcher-level work of the current device and reports
+ * device-side errors (XS_ERR_UNSORTED, XS_ERR_GRID). */
+int xs_launcher_sync(void);
+
+/* ---- 2. engine level ---------------------------------------------------- */
+int xs_engine_create(int device, xs_engine** out);
+int xs_engine_destroy(xs_engine* e);
+/* Stream for all later work of this engine (cudaStream_t; NULL = legacy). */
+int xs_engine_set_stream(xs_engine* e, void* stream);
+/* Waits for the engine's stream and reports device-side errors. */
+int xs_engine_sync(xs_engine* e);
+/* Device bytes held by the engine's scratch (records, windows, counters). */
+int xs_engine_scratch_bytes(xs_engine* e, size_t* bytes);
+/* Upper bound on scratch bytes xs_engine_execute needs for this shape. */
+size_t xs_scratch_bytes_needed(const xs_options* opt, int ncond, size_t n_lines);
+
+/* For each condition c: out[c*out_stride + j] += sigma_c(f_j) for j in
+ * [grid.start_idx, grid.start_idx + grid.points).  Asynchronous on the
+ * engine's stream.  All pointers are device pointers. */
+int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                      const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride);
+
+/* Device time (ms, CUDA events on the engine's stream) of the step-one
+ * (prep) and step-two launches of the last execute; waits for them. */
+int xs_engine_last_stats(xs_engine* e, double* prep_ms, double* steptwo_ms);
+
+/* ---- 3. manager level: BaseManager over host buffers --------------------- */
+/* kind: 0 = GpuManager (reference GPU convention), 1 = OpenMPManager
+ * (reference CPU convention, computed on the GPU). */
+typedef struct xs_manager xs_manager;
+int xs_manager_create(int kind, int profile, int gpu_id, int num_threads, size_t total_memory,
+                      xs_manager** out);
+int xs_manager_destroy(xs_manager* m);
+int xs_manager_set_precision(xs_manager* m, int precision);
+int xs_manager_initialize_vectors(xs_manager* m, int Npoints);
+int xs_manager_initialize_constants(xs_manager* m, double half_width, double temperature,
+                                    double partition, double dfreq, double meanmass,
+                                    double pressure, double ref_temp);
+int xs_manager_transfer_vectors(xs_manager* m, size_t Nener, const double* h_energies,
+                                const double* h_nu, const double* h_aif, const int* h_gns,
+                                const double* h_gamma, const double* h_n);
+int xs_manager_transfer_freq(xs_manager* m, const double* h_freq, const double* h_intens, int N);
+int xs_manager_execute_cross_section(xs_manager* m, int N, int N_ener, int start_idx);
+int xs_manager_transfer_results(xs_manager* m, double* h_freq, double* h_intens, int N);
+int xs_manager_cleanup(xs_manager* m);
+int xs_manager_ready_for_work(xs_manager* m, int* ready);
+int xs_manager_get_ntrans(xs_manager* m, size_t* ntrans);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XSEC_B200_H */
