@@ -1,0 +1,473 @@
+"""Benchmark of the cross-section hot path on B200.
+
+Default workload (one "step"): the batched Voigt sweep -- 1e7 seeded lines,
+grid 500-8000 cm-1 at 0.1 cm-1 (7.5e4 points), the 40 (T, P) conditions
+T in {300..2100 K} x P in {1e-3, 0.1, 1, 10} bar, cut 25 cm-1 -- evaluated in
+mixed precision by one CUDA-graph replay (grid check, step one for all 40
+conditions, persistent step two).  Inputs stay resident in HBM; the per-step
+working set (1e7 lines x 40 conditions of records, ~19 GB) is far larger
+than L2, so no flush is needed between steps.
+
+metric: Voigt line-evals/s = pairs (line, grid point) inside the reference
+window, summed over the 40 conditions, per second of device time.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own 40-condition batch (temperatures shifted
+by rank) with no data-path collective (weak scaling); rank 0 prints one JSON
+line.  --impl reference times the reference's own OpenMPManager (compiled from
+its sources into oracle/_ref/) on the host cores on a bounded sample of the
+same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+FLOPS_PER_PAIR = 14  # algorithmic FLOPs of one Voigt region-I pair
+METRIC = "Voigt line-evals/s (mixed-precision batched 40-(T,P) sweep)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------------
+# workload
+# --------------------------------------------------------------------------
+def sweep_workload(n_lines: int, grid_points: int, rank: int = 0):
+    from gpu_cross_b200 import synth
+
+    lines, grid, conds, common = synth.voigt_sweep_workload(n_lines, grid_points)
+    if rank:
+        conds = [dict(c, temperature=c["temperature"] + 10.0 * rank,
+                      partition=synth.partition_poly(c["temperature"] + 10.0 * rank))
+                 for c in conds]
+    return lines, grid, conds, common
+
+
+def pairs_gpu_window(nu: np.ndarray, freq: np.ndarray, cut: float) -> int:
+    """Pairs with -cut <= nu - f <= cut (the reference GPU window)."""
+    lo = np.searchsorted(freq, nu - cut, side="left")
+    hi = np.searchsorted(freq, nu + cut, side="right")
+    return int(np.sum(hi - lo))
+
+
+def pairs_cpu_window(nu: np.ndarray, f0: float, df: float, npts: int, cut: float) -> int:
+    """Pairs of the reference OpenMPManager window
+    [round((nu-cut-f0)/df), round((nu+cut-f0)/df)) clamped to the grid."""
+    ib = np.clip(np.round((nu - cut - f0) / df), 0, npts)
+    ie = np.clip(np.round((nu + cut - f0) / df), 0, npts)
+    return int(np.sum(np.maximum(ie - ib, 0)))
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        loaded = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# reference CPU (OpenMPManager compiled from the reference sources)
+# --------------------------------------------------------------------------
+def reference_cpu_sample(lines, grid, cond, common, target_s: float = 12.0, threads=None):
+    """Time the reference OpenMPManager on a nu-slice of the line list sized
+    for about target_s seconds; returns (pairs/s, threads, description)."""
+    import oracle
+
+    threads = threads or os.cpu_count() or 1
+    fr = grid.freq()
+    c = dict(temperature=cond["temperature"], partition=cond["partition"],
+             mean_mass=common["mean_mass"], pressure=1.0, ref_temp=common["ref_temp"])
+    cut = 25.0
+    mid = len(lines) // 2
+
+    def run(n):
+        a = max(0, mid - n // 2)
+        part = lines.slice(a, a + n)
+        part.gamma = part.gamma * cond["pressure_atm"]
+        z = np.zeros_like(fr)
+        t = time.perf_counter()
+        oracle.ref_cpu(oracle.VOIGT, fr, z, part, c, grid.dfreq, nthreads=threads)
+        dt = time.perf_counter() - t
+        return pairs_cpu_window(part.nu, fr[0], grid.dfreq, len(fr), cut), dt, part
+
+    n = 20000
+    pairs, dt, part = run(n)
+    while dt < 1.0 and n < len(lines):
+        n = min(len(lines), n * 4)
+        pairs, dt, part = run(n)
+    rate = pairs / dt
+    want = int(n * target_s / max(dt, 1e-3))
+    if want > n * 1.5:
+        n = min(len(lines), want)
+        pairs, dt, part = run(n)
+        rate = pairs / dt
+    desc = (f"reference OpenMPManager (g++ -O3), {threads} threads, one condition "
+            f"(T={cond['temperature']:.0f} K, P={cond['pressure_atm'] / 0.986923:.3g} bar), "
+            f"{len(part)} lines nu {part.nu[0]:.1f}-{part.nu[-1]:.1f} cm-1 of the 1e7-line list, "
+            f"{pairs:.3e} pairs in {dt:.2f} s")
+    return rate, threads, desc
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def run_ours(args, rank, world, dist):
+    import torch
+
+    from gpu_cross_b200 import capi
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    lines, grid, conds, common = sweep_workload(args.lines, args.points, rank)
+    fr = grid.freq()
+    npts = len(fr)
+    nc = len(conds)
+    pairs_per_cond = pairs_gpu_window(lines.nu, fr, 25.0)
+    pairs_step = pairs_per_cond * nc
+    log(f"[bench] rank {rank}: {len(lines)} lines, {npts} points, {nc} conditions, "
+        f"{pairs_step:.3e} line-evals per step")
+
+    keys = ("nu", "energies", "aif", "gns", "gamma", "n")
+    host = {k: torch.from_numpy(np.ascontiguousarray(getattr(lines, k))).pin_memory() for k in keys}
+    d = {k: host[k].to(dev, non_blocking=False) for k in keys}
+    dfr = torch.as_tensor(fr, device=dev)
+    out = torch.zeros((nc, npts), dtype=torch.float64, device=dev)
+    out_f64 = torch.zeros_like(out)
+    stream = torch.cuda.current_stream(dev)
+
+    eng = capi.Engine(dev.index)
+    eng.set_stream(stream.cuda_stream)
+    cc = [capi.make_condition(c["temperature"], c["partition"], 1.0, c["pressure_atm"], c["cut"])
+          for c in conds]
+    L = capi.make_lines(d)
+    G = capi.make_grid(dfr)
+    o_mix = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.MIXED,
+                              ref_temp=common["ref_temp"], points_per_thread=args.P,
+                              warps_per_block=args.W)
+    o_f64 = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.FP64,
+                              ref_temp=common["ref_temp"])
+    g_mix = eng.capture(o_mix, cc, L, G, out.data_ptr(), npts, zero_out=True)
+    eng2 = capi.Engine(dev.index)
+    eng2.set_stream(stream.cuda_stream)
+    g_f64 = eng2.capture(o_f64, cc, L, G, out_f64.data_ptr(), npts, zero_out=True)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # peaks of this GPU (roofline denominators of the FP32/FP64 pipes)
+    peaks = capi.measure_peaks(dev.index)
+
+    # warm-up
+    for _ in range(args.warmup):
+        g_mix.launch(stream.cuda_stream)
+    g_f64.launch(stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+
+    # accuracy of the mixed result against the FP64 sweep (same inputs)
+    g_mix.launch(stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    a = out.cpu().numpy()
+    b = out_f64.cpu().numpy()
+    rel_max, integ_max = 0.0, 0.0
+    for k in range(nc):
+        peak = np.abs(b[k]).max()
+        big = np.abs(b[k]) > 1e-6 * peak
+        rel_max = max(rel_max, float(np.max(np.abs(a[k][big] - b[k][big]) / np.abs(b[k][big]))))
+        integ_max = max(integ_max, abs(a[k].sum() - b[k].sum()) / abs(b[k].sum()))
+
+    # timed region: K mixed sweeps
+    gpu_uuid = None
+    try:
+        gpu_uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        if not gpu_uuid.startswith("GPU-"):
+            gpu_uuid = "GPU-" + gpu_uuid
+    except Exception:
+        gpu_uuid = None
+    clocks = ClockSampler(gpu_uuid)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    step2 = []
+    prep = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        g_mix.launch(stream.cuda_stream)
+        p_ms, s_ms = eng.last_stats()
+        prep.append(p_ms)
+        step2.append(s_ms)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_total = e0.elapsed_time(e1)
+    barrier()
+    clk = clocks.stop()
+    ms_total = max_over_ranks(ms_total)
+    ms_step = ms_total / args.steps
+    value = pairs_step * world / (ms_step * 1e-3)
+
+    # plain FP64 sweep, same workload
+    f64_ms = []
+    for _ in range(max(2, args.steps // 3)):
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        g_f64.launch(stream.cuda_stream)
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+        f64_ms.append(t0.elapsed_time(t1))
+    f64_step = max_over_ranks(float(np.mean(f64_ms)))
+    f64_value = pairs_step * world / (f64_step * 1e-3)
+
+    # end-to-end: pinned host lines -> device, sweep, result -> pinned host
+    out_host = torch.empty((nc, npts), dtype=torch.float64).pin_memory()
+    h2d = sum(int(host[k].numel() * host[k].element_size()) for k in keys)
+    d2h = int(out.numel() * out.element_size())
+    e2e_steps = max(2, args.steps // 2)
+    barrier()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(e2e_steps):
+        for k in keys:
+            d[k].copy_(host[k], non_blocking=True)
+        g_mix.launch(stream.cuda_stream)
+        out_host.copy_(out, non_blocking=True)
+    s1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(s0.elapsed_time(s1) / e2e_steps)
+    e2e_value = pairs_step * world / (e2e_ms * 1e-3)
+
+    step2_ms = float(np.mean(step2))
+    achieved = pairs_step * FLOPS_PER_PAIR / (step2_ms * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("steptwo_mixed_sweep_bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            rate, thr, desc = reference_cpu_sample(lines, grid, conds[26], common,
+                                                   target_s=args.cpu_seconds)
+            cpu = {"value": rate, "unit": "line-evals/s", "cores": thr, "kind": "reference",
+                   "sample": desc}
+        except Exception as exc:  # the reference build is test infrastructure
+            cpu = {"value": None, "unit": "line-evals/s", "cores": 0, "kind": "reference",
+                   "sample": f"not run: {exc}"}
+
+    for gobj in (g_mix, g_f64):
+        gobj.close()
+    eng.close()
+    eng2.close()
+
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC,
+        "value": value,
+        "unit": "line-evals/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 profile / f64 offsets+intensities+tile sums",
+        "data": "synthetic (seeded; no line list ships with the reference)",
+        "config": {
+            "workload": "voigt_sweep_40tp: 1e7 lines, nu U(500,8000), grid 500-8000 cm-1 at 0.1 "
+                        "(7.5e4 points), T 300-2100 K x P {1e-3,0.1,1,10} bar, cut 25 cm-1, "
+                        "mixed precision, one CUDA-graph replay per step",
+            "lines": len(lines), "grid_points": npts, "conditions": nc,
+            "line_evals_per_step": pairs_step,
+            "parallelism": f"{world} rank(s), independent (T,P) batches, no collective",
+            "l2": "inputs larger than L2 (records ~19 GB per step), no flush",
+            "points_per_thread": args.P or 4, "warps_per_block": args.W or 8,
+        },
+        "accuracy_vs_fp64": {"max_rel_above_1e-6_peak": rel_max, "max_integrated_rel": integ_max},
+        "fp64": {"value": f64_value, "ms_per_step": f64_step, "unit": "line-evals/s"},
+        "speedup_mixed_vs_fp64": value / f64_value,
+        "kernel_ms": {"steptwo_mean": step2_ms, "prep_mean": float(np.mean(prep))},
+        "roofline": {
+            "bound": "fp32", "achieved": achieved, "peak": peaks["fp32_tflops"],
+            "unit": "TFLOP/s", "frac": achieved / peaks["fp32_tflops"], "traffic": traffic,
+            "peak_source": "measured (in-repo FP32 FMA probe, xs_measure_peaks, burst)",
+            "flops_per_pair": FLOPS_PER_PAIR,
+            "other_peaks": peaks,
+        },
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "line-evals/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk,
+        "when": datetime.datetime.now(datetime.timezone.utc).isoformat(),
+    }
+
+
+def run_reference(args, rank, world):
+    """The reference's own OpenMPManager on the host cores (bounded sample per
+    step); rank 0 only."""
+    if rank != 0:
+        return None
+    lines, grid, conds, common = sweep_workload(args.lines, args.points, 0)
+    rates = []
+    desc, thr = "", 0
+    for _ in range(args.warmup and 1):
+        reference_cpu_sample(lines, grid, conds[26], common, target_s=min(3.0, args.cpu_seconds))
+    for _ in range(args.steps):
+        rate, thr, desc = reference_cpu_sample(lines, grid, conds[26], common,
+                                               target_s=args.cpu_seconds)
+        rates.append(rate)
+    v = float(np.mean(rates))
+    fr = grid.freq()
+    pairs_step = pairs_gpu_window(lines.nu, fr, 25.0) * len(conds)
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": "line-evals/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": pairs_step / v * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "voigt_sweep_40tp (bounded per-step sample, see cpu_baseline)",
+                   "lines": len(lines), "grid_points": len(fr), "conditions": len(conds)},
+        "cpu_baseline": {"value": v, "unit": "line-evals/s", "cores": thr, "kind": "reference",
+                         "sample": desc},
+        "e2e": {"value": v, "unit": "line-evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--lines", type=int, default=10_000_000)
+    ap.add_argument("--points", type=int, default=75_000)
+    ap.add_argument("--P", type=int, default=0)
+    ap.add_argument("--W", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        log("[bench] warm-up raised to 3")
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    dist = None
+    if world > 1 and args.impl == "ours":
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        res = run_ours(args, rank, world, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if res is not None and rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

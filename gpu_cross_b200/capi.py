@@ -82,6 +82,12 @@ _SIGS = {
     "xs_engine_execute": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _I,
                                ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _SZ]),
     "xs_engine_last_stats": (_I, [_VP, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "xs_engine_capture": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _I,
+                               ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _SZ, _I,
+                               ctypes.POINTER(_VP)]),
+    "xs_graph_launch": (_I, [_VP, _VP]),
+    "xs_graph_destroy": (_I, [_VP]),
+    "xs_measure_peaks": (_I, [_I, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "xs_manager_create": (_I, [_I, _I, _I, _I, _SZ, ctypes.POINTER(_VP)]),
     "xs_manager_destroy": (_I, [_VP]),
     "xs_manager_set_precision": (_I, [_VP, _I]),
@@ -180,10 +186,46 @@ class Engine:
         check(lib().xs_engine_execute(self.h, ctypes.byref(opts), arr, len(conds),
                                       ctypes.byref(lines), ctypes.byref(grid), out_ptr, out_stride))
 
+    def capture(self, opts: Options, conds: list[Condition], lines: Lines, grid: GridC, out_ptr: int,
+                out_stride: int = 0, zero_out: bool = True) -> "Graph":
+        arr = (Condition * len(conds))(*conds)
+        h = ctypes.c_void_p()
+        check(lib().xs_engine_capture(self.h, ctypes.byref(opts), arr, len(conds),
+                                      ctypes.byref(lines), ctypes.byref(grid), out_ptr, out_stride,
+                                      1 if zero_out else 0, ctypes.byref(h)))
+        return Graph(h)
+
     def last_stats(self) -> tuple[float, float]:
         a, b = ctypes.c_double(), ctypes.c_double()
         check(lib().xs_engine_last_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
         return float(a.value), float(b.value)
+
+
+class Graph:
+    """A captured sweep (xs_engine_capture)."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def launch(self, stream_handle: int | None = None) -> None:
+        check(lib().xs_graph_launch(self.h, stream_handle))
+
+    def close(self) -> None:
+        if self.h:
+            lib().xs_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def measure_peaks(device: int = 0) -> dict:
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    check(lib().xs_measure_peaks(device, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+    return dict(fp32_tflops=a.value, fp64_tflops=b.value, rcp32_tops=c.value)
 
 
 def make_lines(dev: dict, count: int | None = None) -> Lines:

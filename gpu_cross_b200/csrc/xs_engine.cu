@@ -353,6 +353,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
         scratch = e->scratch;
     }
+    if (ov && ov->alloc_only) return XS_OK;
     char* base = static_cast<char*>(scratch);
 
     GridDev G;
@@ -404,10 +405,10 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
         pa.mixed_tile_span = 32 * P;
 
-        if (timing && c0 == 0) cudaEventRecord(e->ev[0], st);
+        if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, cudaEventRecordExternal);
         err = launch_prep(kind, opt->convention, mixed, pa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step one launch");
-        if (timing && c0 == 0) cudaEventRecord(e->ev[1], st);
+        if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[1], st, cudaEventRecordExternal);
 
         StepArgs sa;
         std::memset(&sa, 0, sizeof(sa));
@@ -434,7 +435,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         err = launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step two launch");
         if (timing && c0 + nc >= ncond) {
-            cudaEventRecord(e->ev[2], st);
+            cudaEventRecordWithFlags(e->ev[2], st, cudaEventRecordExternal);
             e->timed = true;
         }
     }
@@ -442,3 +443,81 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
 }
 
 }  // namespace xs
+
+struct xs_graph {
+    xs_engine* e = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+int xs_engine_capture(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                      const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride,
+                      int zero_out, xs_graph** out_graph) {
+    if (!e || !out_graph || !grid || !out) return fail(XS_ERR_INVALID, "xs_engine_capture: NULL argument");
+    *out_graph = nullptr;
+    // Grow the scratch outside the capture (allocation is not a stream op).
+    xs::ExecOverride pre;
+    pre.alloc_only = true;
+    int rc = xs::engine_execute(e, opt, conds, ncond, lines, grid, out, out_stride, &pre);
+    if (rc) return rc;
+    DeviceGuard dg(e->device);
+    cudaStream_t cs = nullptr;
+    XS_CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaStream_t saved;
+    {
+        std::lock_guard<std::mutex> lk(e->mu);
+        saved = e->stream;
+        e->stream = cs;
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess && zero_out && grid->points > 0) {
+        const size_t rows = size_t(ncond);
+        const size_t pitch = (ncond > 1 ? out_stride : size_t(grid->npoints_total)) * sizeof(double);
+        err = cudaMemset2DAsync(out + grid->start_idx, pitch, 0, size_t(grid->points) * sizeof(double),
+                                rows, cs);
+    }
+    if (err == cudaSuccess) rc = xs::engine_execute(e, opt, conds, ncond, lines, grid, out, out_stride, nullptr);
+    cudaError_t end = cudaStreamEndCapture(cs, &graph);
+    {
+        std::lock_guard<std::mutex> lk(e->mu);
+        e->stream = saved;
+    }
+    cudaStreamDestroy(cs);
+    if (err != cudaSuccess || end != cudaSuccess || rc != XS_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc != XS_OK) return rc;
+        return cuda_fail(err != cudaSuccess ? err : end, "stream capture");
+    }
+    auto* g = new xs_graph();
+    g->e = e;
+    g->graph = graph;
+    err = cudaGraphInstantiate(&g->exec, graph, 0);
+    if (err != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        delete g;
+        return cuda_fail(err, "cudaGraphInstantiate");
+    }
+    *out_graph = g;
+    return XS_OK;
+}
+
+int xs_graph_launch(xs_graph* g, void* stream) {
+    if (!g) return fail(XS_ERR_INVALID, "xs_graph_launch: NULL graph");
+    DeviceGuard dg(g->e->device);
+    XS_CU(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+    return XS_OK;
+}
+
+int xs_graph_destroy(xs_graph* g) {
+    if (!g) return XS_OK;
+    DeviceGuard dg(g->e->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return XS_OK;
+}
+
+}  // extern "C"

@@ -16,6 +16,7 @@ struct ExecOverride {
     size_t scratch_bytes = 0;
     unsigned* words = nullptr;    // caller-provided error word + counter (device)
     bool no_timing = false;       // skip the CUDA events
+    bool alloc_only = false;      // only grow the engine scratch, launch nothing
     bool use_consts = false;      // take cmcoef and beta from below instead of
     double cmcoef = 0.0;          //   recomputing them from T (launcher level:
     double beta = 0.0;            //   the cross_section_data the caller copied)

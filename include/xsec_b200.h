@@ -180,6 +180,24 @@ int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* c
  * (prep) and step-two launches of the last execute; waits for them. */
 int xs_engine_last_stats(xs_engine* e, double* prep_ms, double* steptwo_ms);
 
+/* Captures one xs_engine_execute (optionally preceded by zeroing the output
+ * rows of the chunk) into a CUDA graph: grid check, step one for every
+ * condition and the persistent step two, replayed by xs_graph_launch on any
+ * stream.  The engine's scratch is sized before the capture; the buffers
+ * named here must stay valid while the graph is used.  xs_engine_last_stats
+ * reports the device times of the most recent replay. */
+typedef struct xs_graph xs_graph;
+int xs_engine_capture(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                      const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride,
+                      int zero_out, xs_graph** graph);
+int xs_graph_launch(xs_graph* graph, void* stream);
+int xs_graph_destroy(xs_graph* graph);
+
+/* Measured throughput of this device's FP32 FMA and FP64 FMA pipes
+ * (TFLOP/s) and of the FP32 reciprocal (MUFU, Tops/s); the roofline
+ * denominators of the step-two kernels. */
+int xs_measure_peaks(int device, double* fp32_tflops, double* fp64_tflops, double* rcp32_tops);
+
 /* ---- 3. manager level: BaseManager over host buffers --------------------- */
 /* kind: 0 = GpuManager (reference GPU convention), 1 = OpenMPManager
  * (reference CPU convention, computed on the GPU). */
