@@ -191,6 +191,9 @@ def run_ours(args, rank, world, dist):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     lines, grid, conds, common = sweep_workload(args.lines, args.points, rank)
+    if args.conds < len(conds):
+        step = len(conds) / float(args.conds)
+        conds = [conds[int(k * step)] for k in range(args.conds)]
     fr = grid.freq()
     npts = len(fr)
     nc = len(conds)
@@ -204,7 +207,7 @@ def run_ours(args, rank, world, dist):
     d = {k: host[k].to(dev, non_blocking=False) for k in keys}
     dfr = torch.as_tensor(fr, device=dev)
     out = torch.zeros((nc, npts), dtype=torch.float64, device=dev)
-    out_f64 = torch.zeros_like(out)
+    out_f64 = torch.zeros_like(out) if not args.no_fp64 else None
     stream = torch.cuda.current_stream(dev)
 
     eng = capi.Engine(dev.index)
@@ -219,9 +222,11 @@ def run_ours(args, rank, world, dist):
     o_f64 = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.FP64,
                               ref_temp=common["ref_temp"])
     g_mix = eng.capture(o_mix, cc, L, G, out.data_ptr(), npts, zero_out=True)
-    eng2 = capi.Engine(dev.index)
-    eng2.set_stream(stream.cuda_stream)
-    g_f64 = eng2.capture(o_f64, cc, L, G, out_f64.data_ptr(), npts, zero_out=True)
+    eng2 = g_f64 = None
+    if not args.no_fp64:
+        eng2 = capi.Engine(dev.index)
+        eng2.set_stream(stream.cuda_stream)
+        g_f64 = eng2.capture(o_f64, cc, L, G, out_f64.data_ptr(), npts, zero_out=True)
 
     def barrier():
         if dist is not None:
@@ -241,16 +246,17 @@ def run_ours(args, rank, world, dist):
     # warm-up
     for _ in range(args.warmup):
         g_mix.launch(stream.cuda_stream)
-    g_f64.launch(stream.cuda_stream)
+    if g_f64 is not None:
+        g_f64.launch(stream.cuda_stream)
     torch.cuda.synchronize(dev)
 
     # accuracy of the mixed result against the FP64 sweep (same inputs)
     g_mix.launch(stream.cuda_stream)
     torch.cuda.synchronize(dev)
     a = out.cpu().numpy()
-    b = out_f64.cpu().numpy()
+    b = out_f64.cpu().numpy() if out_f64 is not None else a
     rel_max, integ_max = 0.0, 0.0
-    for k in range(nc):
+    for k in range(nc if out_f64 is not None else 0):
         peak = np.abs(b[k]).max()
         big = np.abs(b[k]) > 1e-6 * peak
         rel_max = max(rel_max, float(np.max(np.abs(a[k][big] - b[k][big]) / np.abs(b[k][big]))))
@@ -289,7 +295,7 @@ def run_ours(args, rank, world, dist):
 
     # plain FP64 sweep, same workload
     f64_ms = []
-    for _ in range(max(2, args.steps // 3)):
+    for _ in range(max(2, args.steps // 3) if g_f64 is not None else 0):
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
@@ -297,14 +303,14 @@ def run_ours(args, rank, world, dist):
         t1.record(stream)
         torch.cuda.synchronize(dev)
         f64_ms.append(t0.elapsed_time(t1))
-    f64_step = max_over_ranks(float(np.mean(f64_ms)))
-    f64_value = pairs_step * world / (f64_step * 1e-3)
+    f64_step = max_over_ranks(float(np.mean(f64_ms))) if f64_ms else float("nan")
+    f64_value = pairs_step * world / (f64_step * 1e-3) if f64_ms else None
 
     # end-to-end: pinned host lines -> device, sweep, result -> pinned host
     out_host = torch.empty((nc, npts), dtype=torch.float64).pin_memory()
     h2d = sum(int(host[k].numel() * host[k].element_size()) for k in keys)
     d2h = int(out.numel() * out.element_size())
-    e2e_steps = max(2, args.steps // 2)
+    e2e_steps = 0 if args.no_e2e else max(2, args.steps // 2)
     barrier()
     s0 = torch.cuda.Event(enable_timing=True)
     s1 = torch.cuda.Event(enable_timing=True)
@@ -316,8 +322,8 @@ def run_ours(args, rank, world, dist):
         out_host.copy_(out, non_blocking=True)
     s1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = max_over_ranks(s0.elapsed_time(s1) / e2e_steps)
-    e2e_value = pairs_step * world / (e2e_ms * 1e-3)
+    e2e_ms = max_over_ranks(s0.elapsed_time(s1) / e2e_steps) if e2e_steps else float("nan")
+    e2e_value = pairs_step * world / (e2e_ms * 1e-3) if e2e_steps else None
 
     step2_ms = float(np.mean(step2))
     achieved = pairs_step * FLOPS_PER_PAIR / (step2_ms * 1e-3) / 1e12
@@ -341,9 +347,11 @@ def run_ours(args, rank, world, dist):
                    "sample": f"not run: {exc}"}
 
     for gobj in (g_mix, g_f64):
-        gobj.close()
+        if gobj is not None:
+            gobj.close()
     eng.close()
-    eng2.close()
+    if eng2 is not None:
+        eng2.close()
 
     if rank != 0:
         return None
@@ -372,7 +380,7 @@ def run_ours(args, rank, world, dist):
         },
         "accuracy_vs_fp64": {"max_rel_above_1e-6_peak": rel_max, "max_integrated_rel": integ_max},
         "fp64": {"value": f64_value, "ms_per_step": f64_step, "unit": "line-evals/s"},
-        "speedup_mixed_vs_fp64": value / f64_value,
+        "speedup_mixed_vs_fp64": value / f64_value if f64_value else None,
         "kernel_ms": {"steptwo_mean": step2_ms, "prep_mean": float(np.mean(prep))},
         "roofline": {
             "bound": "fp32", "achieved": achieved, "peak": peaks["fp32_tflops"],
@@ -441,6 +449,9 @@ def main():
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--W", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--conds", type=int, default=40, help="subset of the 40 conditions (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

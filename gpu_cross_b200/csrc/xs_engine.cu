@@ -375,6 +375,15 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
 
     const cudaStream_t st = e->stream;
     const bool timing = !(ov && ov->no_timing);
+    // Inside a stream capture the timing events must become event-record
+    // nodes of the graph (cudaEventRecordExternal); outside one, a plain
+    // record (the external flag is refused there).
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        cap = cudaStreamCaptureStatusNone;
+    }
+    const unsigned ev_flags = (cap == cudaStreamCaptureStatusActive) ? cudaEventRecordExternal : 0u;
     cudaError_t err = launch_grid_check(G, words, st);
     if (err != cudaSuccess) return cuda_fail(err, "grid check launch");
 
@@ -405,10 +414,10 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
         pa.mixed_tile_span = 32 * P;
 
-        if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, cudaEventRecordExternal);
+        if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, ev_flags);
         err = launch_prep(kind, opt->convention, mixed, pa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step one launch");
-        if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[1], st, cudaEventRecordExternal);
+        if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[1], st, ev_flags);
 
         StepArgs sa;
         std::memset(&sa, 0, sizeof(sa));
@@ -435,7 +444,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         err = launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step two launch");
         if (timing && c0 + nc >= ncond) {
-            cudaEventRecordWithFlags(e->ev[2], st, cudaEventRecordExternal);
+            cudaEventRecordWithFlags(e->ev[2], st, ev_flags);
             e->timed = true;
         }
     }
