@@ -88,6 +88,8 @@ _SIGS = {
     "xs_graph_launch": (_I, [_VP, _VP]),
     "xs_graph_destroy": (_I, [_VP]),
     "xs_measure_peaks": (_I, [_I, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "xs_execute_noalloc": (_I, [ctypes.POINTER(Options), ctypes.POINTER(Condition),
+                                ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _VP]),
     "xs_manager_create": (_I, [_I, _I, _I, _I, _SZ, ctypes.POINTER(_VP)]),
     "xs_manager_destroy": (_I, [_VP]),
     "xs_manager_set_precision": (_I, [_VP, _I]),

@@ -27,6 +27,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
                    const ExecOverride* ov);
 
 int set_error(int code, const char* msg);
+CondDev make_cond(const xs_options& o, const xs_condition& c);
 long cpu_covered_lines(long n, int threads);
 
 }  // namespace xs

@@ -198,6 +198,29 @@ int xs_graph_destroy(xs_graph* graph);
  * denominators of the step-two kernels. */
 int xs_measure_peaks(int device, double* fp32_tflops, double* fp64_tflops, double* rcp32_tops);
 
+/* Allocation-free variant of xs_engine_execute for ONE condition.  It has no
+ * counterpart in the reference.  For callers that cannot let this library
+ * allocate device memory: a host whose own pool allocator already holds the
+ * device's memory (a cudaMalloc here would fail or shrink that pool), or a
+ * latency-critical loop that cannot take the device-wide synchronisation
+ * cudaMalloc/cudaFree may cause.  Inputs and outputs are the caller's
+ * (device pointers, as for xs_engine_execute with ncond = 1 and `out`
+ * accumulated); the scratch is one fixed array of XS_NOALLOC_SCRATCH_BYTES
+ * compiled into the library, which every GPU that loads the library holds
+ * until the process exits.  Line counts whose scratch would not fit (about
+ * 320,000 lines for FP64 Voigt, 380,000 for mixed Voigt, 690,000 for
+ * Doppler/Gaussian) are rejected with XS_ERR_INVALID before any device work.
+ * The first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture.  Work is
+ * enqueued on `stream` (cudaStream_t; NULL = legacy) and the call waits for
+ * it, then reports XS_ERR_UNSORTED / XS_ERR_GRID like xs_engine_sync.  Every
+ * call shares the one array and it keeps the previous call's contents; calls
+ * that overlap on the GPU (e.g. issued from two host threads at once) race on
+ * it -- serialise them. */
+#define XS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int xs_execute_noalloc(const xs_options* opt, const xs_condition* cond, const xs_lines* lines,
+                       const xs_grid* grid, double* out, void* stream);
+
 /* ---- 3. manager level: BaseManager over host buffers --------------------- */
 /* kind: 0 = GpuManager (reference GPU convention), 1 = OpenMPManager
  * (reference CPU convention, computed on the GPU). */
