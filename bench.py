@@ -48,10 +48,17 @@ def log(*a):
 # --------------------------------------------------------------------------
 # workload
 # --------------------------------------------------------------------------
-def sweep_workload(n_lines: int, grid_points: int, rank: int = 0):
+def sweep_workload(n_lines: int, grid_points: int, rank: int = 0, workload: str = "sweep"):
     from gpu_cross_b200 import synth
 
-    lines, grid, conds, common = synth.voigt_sweep_workload(n_lines, grid_points)
+    if workload == "single":
+        # Voigt single point: T = 1000 K, P = 1 bar, grid 500-8000 at 0.01
+        lines, grid, cond = synth.voigt_single_workload(n_lines, grid_points)
+        conds = [dict(temperature=cond["temperature"], partition=cond["partition"],
+                      pressure_atm=1.0, cut=25.0)]
+        common = dict(mean_mass=cond["mean_mass"], ref_temp=cond["ref_temp"])
+    else:
+        lines, grid, conds, common = synth.voigt_sweep_workload(n_lines, grid_points)
     if rank:
         conds = [dict(c, temperature=c["temperature"] + 10.0 * rank,
                       partition=synth.partition_poly(c["temperature"] + 10.0 * rank))
@@ -190,7 +197,7 @@ def run_ours(args, rank, world, dist):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    lines, grid, conds, common = sweep_workload(args.lines, args.points, rank)
+    lines, grid, conds, common = sweep_workload(args.lines, args.points, rank, args.workload)
     if args.conds < len(conds):
         step = len(conds) / float(args.conds)
         conds = [conds[int(k * step)] for k in range(args.conds)]
@@ -338,7 +345,7 @@ def run_ours(args, rank, world, dist):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            rate, thr, desc = reference_cpu_sample(lines, grid, conds[26], common,
+            rate, thr, desc = reference_cpu_sample(lines, grid, conds[min(26, len(conds) - 1)], common,
                                                    target_s=args.cpu_seconds)
             cpu = {"value": rate, "unit": "line-evals/s", "cores": thr, "kind": "reference",
                    "sample": desc}
@@ -407,9 +414,9 @@ def run_reference(args, rank, world):
     rates = []
     desc, thr = "", 0
     for _ in range(args.warmup and 1):
-        reference_cpu_sample(lines, grid, conds[26], common, target_s=min(3.0, args.cpu_seconds))
+        reference_cpu_sample(lines, grid, conds[min(26, len(conds) - 1)], common, target_s=min(3.0, args.cpu_seconds))
     for _ in range(args.steps):
-        rate, thr, desc = reference_cpu_sample(lines, grid, conds[26], common,
+        rate, thr, desc = reference_cpu_sample(lines, grid, conds[min(26, len(conds) - 1)], common,
                                                target_s=args.cpu_seconds)
         rates.append(rate)
     v = float(np.mean(rates))
@@ -445,7 +452,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--lines", type=int, default=10_000_000)
-    ap.add_argument("--points", type=int, default=75_000)
+    ap.add_argument("--points", type=int, default=0, help="grid points (default per workload)")
+    ap.add_argument("--workload", choices=["sweep", "single"], default="sweep")
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--W", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -454,6 +462,8 @@ def main():
     ap.add_argument("--conds", type=int, default=40, help="subset of the 40 conditions (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
+    if not args.points:
+        args.points = 750_000 if args.workload == "single" else 75_000
     if args.warmup < 3 and args.impl == "ours":
         log("[bench] warm-up raised to 3")
         args.warmup = 3

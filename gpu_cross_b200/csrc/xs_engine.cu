@@ -56,8 +56,6 @@ struct DeviceGuard {
     }
 };
 
-size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-
 }  // namespace
 
 struct xs_engine {
@@ -236,9 +234,8 @@ int xs_engine_scratch_bytes(xs_engine* e, size_t* bytes) {
 size_t xs_scratch_bytes_needed(const xs_options* opt, int ncond, size_t n_lines) {
     if (!opt || ncond < 1) return 0;
     const bool mixed = opt->profile == XS_VOIGT && opt->precision == XS_MIXED;
-    const size_t per = record_bytes(opt->profile, mixed) + aux_bytes(opt->profile, mixed) + 2 * sizeof(int);
     const int nc = ncond < kMaxCond ? ncond : kMaxCond;
-    return align_up(per * n_lines * size_t(nc) + 4 * 256, 256);
+    return plan_scratch(opt->profile, mixed, n_lines, nc, 0).need;
 }
 
 int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
@@ -322,14 +319,9 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     DeviceGuard dg(e->device);
 
     // Scratch layout for one group of conditions.
-    const size_t rb = record_bytes(kind, mixed), ab = aux_bytes(kind, mixed);
     const int group = ncond < kMaxCond ? ncond : kMaxCond;
-    const size_t nl = size_t(n);
-    const size_t off_rec = 0;
-    const size_t off_aux = align_up(off_rec + rb * nl * group, 256);
-    const size_t off_wlo = align_up(off_aux + ab * nl * group, 256);
-    const size_t off_whi = align_up(off_wlo + sizeof(int) * nl * group, 256);
-    const size_t need = align_up(off_whi + sizeof(int) * nl * group, 256);
+    const ScratchPlan plan = plan_scratch(kind, mixed, size_t(n), group, 0);
+    const size_t need = plan.need;
 
     void* scratch = nullptr;
     unsigned* words = e->d_words;
@@ -401,10 +393,11 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
                 pa.cond[c].beta = ov->beta;
             }
         }
-        pa.rec = base + off_rec;
-        pa.aux = ab ? base + off_aux : nullptr;
-        pa.wlo = reinterpret_cast<int*>(base + off_wlo);
-        pa.whi = reinterpret_cast<int*>(base + off_whi);
+        pa.rec = base + plan.off_rec;
+        pa.wlo = reinterpret_cast<int*>(base + plan.off_wlo);
+        pa.whi = reinterpret_cast<int*>(base + plan.off_whi);
+        pa.mi = reinterpret_cast<int*>(base + plan.off_mi);
+        pa.kc = reinterpret_cast<int*>(base + plan.off_kc);
         pa.err = words;
         pa.half_width = opt->half_width;
         pa.x0 = opt->dfreq * 0.5;
@@ -415,6 +408,8 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.mixed_tile_span = 32 * P;
 
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, ev_flags);
+        err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(kMaxCond), st);
+        if (err != cudaSuccess) return cuda_fail(err, "core-width reset");
         err = launch_prep(kind, opt->convention, mixed, pa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step one launch");
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[1], st, ev_flags);
@@ -422,9 +417,10 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         StepArgs sa;
         std::memset(&sa, 0, sizeof(sa));
         sa.rec = pa.rec;
-        sa.aux = static_cast<const AuxV64*>(pa.aux);
         sa.wlo = pa.wlo;
         sa.whi = pa.whi;
+        sa.mi = pa.mi;
+        sa.kc = pa.kc;
         sa.n = n;
         sa.out = out + size_t(c0) * out_stride;
         sa.out_stride = out_stride;

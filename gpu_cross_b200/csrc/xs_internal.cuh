@@ -52,33 +52,37 @@ struct CondDev {
     double pad;
 };
 
-// Voigt FP64 record, one per (line, condition).  Region I of W4 written as
-// a real rational in x^2: Re w * pref = (Pc x^2 + Qc) / (x^2 (x^2 + B) + A2)
-// with Pc = pref c y, Qc = Pc (0.5 + y^2), B = 2 y^2 - 1, A2 = (0.5 + y^2)^2.
+// Voigt records, one per (line, condition).  Region I of W4,
+// Re[T c / (0.5 + T^2)] with T = y - ix, is evaluated as
+//   Re w * pref = Pc (u + 1) / (u^2 + D2),  u = x^2 + Cy,
+// with Cy = y^2 - 0.5, D2 = 2 y^2, Pc = pref c y (c = 0.5641896): the same
+// rational as c y (0.5 + x^2 + y^2) / ((0.5 + y^2 - x^2)^2 + 4 x^2 y^2), since
+// (0.5 + y^2 - x^2)^2 + 4 x^2 y^2 = (x^2 + y^2 - 0.5)^2 + 2 y^2.  In region I
+// (|x| + y >= 15) u > 190, so nothing cancels.
+// FP64 record: the first three 16-byte chunks are all the fast path reads.
 struct __align__(16) RecV64 {
-    double nu;   // line centre used for offsets
-    double g;    // 1 / Doppler width
-    double B, A2, Pc, Qc;
+    double nu;     // line centre used for offsets
+    double g;      // 1 / Doppler width
+    double Cy, D2;
+    double Pc, y;  // y = Lorentz / Doppler width ratio
+    double pref;   // S * g
+    double pad;
     int lo, hi;    // window [lo, hi) of grid indices
     int clo, chi;  // grid indices near the core (region I not guaranteed)
 };
-static_assert(sizeof(RecV64) == 64, "RecV64 layout");
+static_assert(sizeof(RecV64) == 80, "RecV64 layout");
 
-// FP64 data for the exact (slow) path of a Voigt pair.
-struct __align__(16) AuxV64 {
-    double nu, g, y, pref;  // pref = S * g
-};
-static_assert(sizeof(AuxV64) == 32, "AuxV64 layout");
-
-// Voigt mixed-precision record (FP32).  The offset of grid point j from the
-// line centre is (m - j) * df + r in cm-1, with m the nearest grid index and
+// Mixed-precision record (FP32).  The offset of grid point j from the line
+// centre is (m - j) * df + r in cm-1, with m the nearest grid index and
 // |r| <= df/2 computed in FP64; stored scaled by g: x = (m - j) * dfa + ra.
+// The first two 16-byte chunks are all the fast path reads.
 struct __align__(16) RecV32 {
-    float m, ra, dfa, B;
-    float A2, Pc, Qc, y;
+    float m, ra, dfa, Cy;
+    float D2, Pc, pref, y;
     float lo, hi, clo, chi;
+    float pad0, pad1, pad2, pad3;
 };
-static_assert(sizeof(RecV32) == 48, "RecV32 layout");
+static_assert(sizeof(RecV32) == 64, "RecV32 layout");
 
 // Doppler / Gaussian record (FP64).
 struct __align__(16) RecE64 {
@@ -110,9 +114,10 @@ struct PrepArgs {
     int ncond;
     CondDev cond[kMaxCond];
     void* rec;          // records, condition-major: rec + c * n
-    void* aux;          // AuxV64 (Voigt only)
     int* wlo;           // windows, condition-major
     int* whi;
+    int* mi;            // nearest grid index of each line (condition-free)
+    int* kc;            // per condition: max core half-width in grid points
     unsigned* err;
     double half_width;  // Gaussian
     double x0;          // Doppler half bin: dfreq * 0.5
@@ -122,9 +127,10 @@ struct PrepArgs {
 
 struct StepArgs {
     const void* rec;
-    const AuxV64* aux;
     const int* wlo;
     const int* whi;
+    const int* mi;
+    const int* kc;
     long n;             // lines per condition
     double* out;
     size_t out_stride;  // elements between conditions
@@ -144,6 +150,13 @@ cudaError_t launch_steptwo(int kind, int conv, bool mixed, int P, int warps, int
 // Resident blocks per SM for a step-two configuration.
 int steptwo_blocks_per_sm(int kind, int conv, bool mixed, int P, int warps);
 size_t record_bytes(int kind, bool mixed);
-size_t aux_bytes(int kind, bool mixed);
+
+// Layout of the scratch one execute call needs: records and windows for
+// `ncond` conditions of `n` lines, the per-line grid index and the
+// per-condition core widths; sections 256-byte aligned from `base_off`.
+struct ScratchPlan {
+    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, need;
+};
+ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off);
 
 }  // namespace xs

@@ -33,7 +33,6 @@ namespace {
 struct cplx {
     double re, im;
 };
-__device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
 __device__ __forceinline__ cplx operator+(double a, cplx b) { return {a + b.re, b.im}; }
 __device__ __forceinline__ cplx operator-(double a, cplx b) { return {a - b.re, -b.im}; }
 __device__ __forceinline__ cplx operator*(cplx a, cplx b) {
@@ -124,11 +123,9 @@ __global__ void k_grid_check(GridDev g, unsigned* err) {
 // ---------------------------------------------------------------------------
 // Step one.
 // ---------------------------------------------------------------------------
+// Returns the line's core half-width in grid points (Voigt; 0 otherwise).
 template <int KIND, int CONV, bool MIXED>
-__global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int c = blockIdx.y;
-    if (i >= a.L.n) return;
+__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c) {
     const CondDev& C = a.cond[c];
     const double* F = a.G.freq;
     const double f0 = F[0];
@@ -141,6 +138,7 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
     const double gns = double(a.L.gns[i]);
     const double cut = C.cut;
     const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
+    int kcl = 0;
 
     // Intensity, centre used for offsets, and the reference window.
     double S, nu_p;
@@ -201,9 +199,9 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
         const double pref = (CONV == kConvCpu && S == 0.0) ? 0.0 : S * g;
         const double y2 = y * y;
         const double Pc = pref * kW4C * y;
-        const double Qc = Pc * (0.5 + y2);
-        const double B = 2.0 * y2 - 1.0;
-        const double A2 = (0.5 + y2) * (0.5 + y2);
+        const double Cy = y2 - 0.5;
+        const double D2 = 2.0 * y2;
+        const double m = rint((nu_p - f0) / df);
         // Grid indices where |x| + y < 15 is possible (region I not
         // guaranteed), with a margin of two points either side.
         double clo_d = 3.0e7, chi_d = -3.0e7;
@@ -215,39 +213,48 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
             if (!(clo_d > -3.0e7)) clo_d = -3.0e7;
             if (!(chi_d < 3.0e7)) chi_d = 3.0e7;
         }
-        AuxV64* aux = reinterpret_cast<AuxV64*>(a.aux) + ci;
-        *aux = AuxV64{nu_p, g, y, pref};
+        // FP32 offsets need |m| < 2^24 and x below ~1e8 over the window;
+        // otherwise every pair of the line takes the per-pair path.
+        bool whole = false;
         if (MIXED) {
-            const double m = rint((nu_p - f0) / df);
-            const double r = (nu_p - f0) - m * df;
-            // FP32 offsets need |m| < 2^24 and x below ~1e8 over the window.
             const double xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
-            if (!(fabs(m) < 16000000.0) || !(xw < 1.0e8)) {
-                clo_d = -3.0e7;
-                chi_d = 3.0e7;
-            }
+            whole = !(fabs(m) < 16000000.0) || !(xw < 1.0e8);
+        }
+        if (whole) {
+            clo_d = -3.0e7;
+            chi_d = 3.0e7;
+            kcl = 30000000;
+        } else if (chi_d >= clo_d) {
+            const double w = fmax(m - clo_d, chi_d - m) + 1.0;
+            kcl = w < 3.0e7 ? int(w) : 30000000;
+        }
+        if (c == 0) a.mi[i] = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
+        if (MIXED) {
             RecV32 rr;
             rr.m = float(fabs(m) < 16000000.0 ? m : 0.0);
-            rr.ra = float(r * g);
+            rr.ra = float(((nu_p - f0) - m * df) * g);
             rr.dfa = float(df * g);
-            rr.B = float(B);
-            rr.A2 = float(A2);
+            rr.Cy = float(Cy);
+            rr.D2 = float(D2);
             rr.Pc = float(Pc);
-            rr.Qc = float(Qc);
+            rr.pref = float(pref);
             rr.y = float(y);
             rr.lo = float(lo);
             rr.hi = float(hi);
             rr.clo = float(clo_d);
             rr.chi = float(chi_d);
+            rr.pad0 = rr.pad1 = rr.pad2 = rr.pad3 = 0.0f;
             reinterpret_cast<RecV32*>(a.rec)[ci] = rr;
         } else {
             RecV64 rr;
             rr.nu = nu_p;
             rr.g = g;
-            rr.B = B;
-            rr.A2 = A2;
+            rr.Cy = Cy;
+            rr.D2 = D2;
             rr.Pc = Pc;
-            rr.Qc = Qc;
+            rr.y = y;
+            rr.pref = pref;
+            rr.pad = 0.0;
             rr.lo = lo;
             rr.hi = hi;
             rr.clo = int(clo_d);
@@ -286,6 +293,27 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
     }
     a.wlo[ci] = lo;
     a.whi[ci] = hi;
+    return kcl;
+}
+
+template <int KIND, int CONV, bool MIXED>
+__global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    int kcl = 0;
+    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c);
+    if (KIND == kVoigt) {
+        // Block maximum of the core widths, one atomic per block.
+        __shared__ int smax[8];
+        kcl = __reduce_max_sync(0xffffffffu, kcl);
+        if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = kcl;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int m = 0;
+            for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[w] > m ? smax[w] : m;
+            if (m > 0) atomicMax(a.kc + c, m);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -362,26 +390,212 @@ __device__ __forceinline__ bool next_item(const StepArgs& a, int P, int lane, Wo
 // ---------------------------------------------------------------------------
 // Step two, Voigt.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float rcp_approx_f32(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// 1/x: the hardware approximation refined by one Newton-Raphson step
+// (r <- r + r (1 - x r)), which squares its relative error.
+__device__ __forceinline__ double rcp_refined_f64(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    const double e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
+struct fcplx {
+    float re, im;
+};
+__device__ __forceinline__ fcplx operator+(float a, fcplx b) { return {a + b.re, b.im}; }
+__device__ __forceinline__ fcplx operator*(fcplx a, fcplx b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+// W4 region II (5.5 <= |x| + y < 15) as a real expression with the factor y
+// explicit.  With T = y - ix, U = T^2 = Ur + i Ui, N = a + b U and
+// D = c + U (3 + U):
+//   Re[T N / D] = y [(a + b y^2 - 3 b x^2) Dr + 2 x^2 (3 + 2 Ur)(Nr + 2 b y^2)] / |D|^2
+// (expanding Re[T N conj(D)]); a complex evaluation would cancel by a factor
+// x / y in the wings of narrow lines.
+template <class R>
+__device__ __forceinline__ R w4_region2_re(R x, R y) {
+    const R a = R(1.410474), b = R(.5641896), c = R(.75);
+    const R x2 = x * x, y2 = y * y;
+    const R ur = y2 - x2, ui = R(-2) * x * y;
+    const R nr = a + b * ur;
+    const R dr = c + R(3) * ur + ur * ur - ui * ui;
+    const R di = ui * (R(3) + R(2) * ur);
+    const R br = (a + b * y2 - R(3) * b * x2) * dr + R(2) * x2 * (R(3) + R(2) * ur) * (nr + R(2) * b * y2);
+    return y * br / (dr * dr + di * di);
+}
+
+// W4 region III in FP32 (there y >= 0.195|x| - 0.176, so Re w is not small
+// next to |w| and the complex form keeps its accuracy).
+__device__ __forceinline__ float w4_region3_re_f32(float x, float y) {
+    const fcplx t = {y, -x};
+    const fcplx num = 16.4955f + t * (20.20933f + t * (11.96482f + t * (3.778987f + t * fcplx{.5642236f, 0.f})));
+    const fcplx den = 16.4955f + t * (38.82363f + t * (39.27121f + t * (21.69274f + t * (6.699398f + t))));
+    return (num.re * den.re + num.im * den.im) / (den.re * den.re + den.im * den.im);
+}
+
+// W4 region IV in FP64 (exp(U) minus a rational cancel for small y).
+__device__ double w4_region4_re(double x, double y) {
+    const cplx t = {y, -x};
+    const cplx u = t * t;
+    double sn, cs;
+    sincos(u.im, &sn, &cs);
+    const double eu = exp(u.re);
+    const cplx num =
+        36183.31 - u * (3321.9905 - u * (1540.787 - u * (219.0313 - u * (35.76683 - u * (1.320522 - u * .56419)))));
+    const cplx den =
+        32066.6 - u * (24322.84 - u * (9022.228 - u * (2186.181 - u * (364.2191 - u * (61.57037 - u * (1.841439 - u))))));
+    return eu * cs - div_re(t * num, den);
+}
+
+// W4 region IV for the mixed path: exp(U) = exp(y^2 - x^2) cos(2xy) + i(...)
+// has no cancellation and is taken in FP32; the rational T P(U) / Q(U), whose
+// real part is O(y) and computed through cancelling complex products, in
+// FP64.
+__device__ float w4_region4_re_mixed(float x, float y) {
+    const float e = expf(fmaf(y, y, -x * x)) * cosf(2.0f * x * y);
+    const cplx t = {double(y), -double(x)};
+    const cplx u = t * t;
+    const cplx num =
+        36183.31 - u * (3321.9905 - u * (1540.787 - u * (219.0313 - u * (35.76683 - u * (1.320522 - u * .56419)))));
+    const cplx den =
+        32066.6 - u * (24322.84 - u * (9022.228 - u * (2186.181 - u * (364.2191 - u * (61.57037 - u * (1.841439 - u))))));
+    return e - float(div_re(t * num, den));
+}
+
+// Persistent step two.  For a tile [t0, t1) the lines [La, Lb) meet it;
+// since the window bounds lo[] and hi[] are ascending in line order, the
+// lines covering the whole tile form one contiguous run [fs, fe), and among
+// those the ones whose core may reach the tile ([E, F), from the ascending
+// nearest-grid-index array mi[] and the condition's widest core kc) form
+// another.  So every staged group splits into at most five contiguous runs:
+//   partial [La, fs) | fast [fs, E) | core [E, F) | fast [F, fe) | partial [fe, Lb)
+// Fast lines evaluate W4 region I on every pair with no test at all.  Core
+// and partial lines classify whole rows (outside the window: skipped; inside
+// and clear of the core band: as fast; otherwise lane by lane).  Pairs that
+// need W4 regions II-IV are not evaluated in place -- that would run the
+// union of the region code paths with a few lanes active -- but pushed to a
+// per-warp queue in shared memory and evaluated 32 at a time, one per lane;
+// each lane then adds the results addressed to it, in queue order, to a
+// per-lane correction column.  The order of every sum is fixed.
+template <class T>
+struct CoreEntry {
+    T x, y, pref;
+    int dest;  // lane | (row << 5)
+};
+
+template <int P, bool MIXED>
+struct WarpCoreQueue {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    static constexpr int kCap = 32 * (P + 1);  // < 32 left + up to P rows of 32
+    CoreEntry<T> q[kCap];
+    T val[32];
+    T corr[P][32];
+};
+
+// Evaluates the first k (<= 32) queued pairs, one per lane, adds each result
+// to its destination lane's correction column in queue order, and moves the
+// rest of the queue to the front.  Returns the new queue length.  Kept out of
+// line: it runs once per 32 pairs and holds all of W4's regions II-IV.
+template <int P, bool MIXED>
+__device__ __noinline__ int core_queue_flush(WarpCoreQueue<P, MIXED>& cq, int qn, int k, int lane) {
+    using T = typename WarpCoreQueue<P, MIXED>::T;
+    T v = T(0);
+    if (lane < k) {
+        const CoreEntry<T> e = cq.q[lane];
+        if (MIXED) {
+            // only regions III and IV are queued on the mixed path
+            const float ax = float(e.x), y = float(e.y);
+            const float w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y)
+                                                             : w4_region4_re_mixed(ax, y);
+            v = T(float(e.pref) * w);
+        } else {
+            v = T(w4_re(double(e.x), double(e.y)) * double(e.pref));
+        }
+    }
+    cq.val[lane] = v;
+    __syncwarp();
+    for (int i = 0; i < k; ++i) {
+        const int d = cq.q[i].dest;
+        if ((d & 31) == lane) cq.corr[d >> 5][lane] += cq.val[i];
+    }
+    __syncwarp();
+    const int rem = qn - k;
+    for (int base = 0; base < rem; base += 32) {
+        CoreEntry<T> keep;
+        const int i = base + lane;
+        if (i < rem) keep = cq.q[k + i];
+        __syncwarp();
+        if (i < rem) cq.q[i] = keep;
+        __syncwarp();
+    }
+    return rem;
+}
+
+// Resident blocks per SM the step-two Voigt kernel asks the compiler to fit
+// (register budget): 24 warps per SM for the FP32 path up to 4 points per
+// thread.
 template <int P, int WARPS, bool MIXED>
-__global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt(StepArgs a) {
+constexpr int voigt_min_blocks() {
+    return (MIXED && P <= 4) ? 24 / WARPS : 1;
+}
+
+template <int P, int WARPS, bool MIXED>
+__global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>()))
+    k_steptwo_voigt(StepArgs a) {
     using REC = typename std::conditional<MIXED, RecV32, RecV64>::type;
+    using T = typename std::conditional<MIXED, float, double>::type;
+    using Q = WarpCoreQueue<P, MIXED>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     REC* buf = reinterpret_cast<REC*>(smem_raw) + warp * 64;
+    Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 64 * sizeof(REC))[warp];
     const REC* recs_all = reinterpret_cast<const REC*>(a.rec);
     const double* F = a.G.freq;
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+#pragma unroll
+    for (int p = 0; p < P; ++p) cq.corr[p][lane] = T(0);
+    int qn = 0;  // entries in the queue (warp-uniform)
+
+    auto push = [&](bool need, T x, T y, T pref, int p) {
+        const unsigned b = __ballot_sync(0xffffffffu, need);
+        if (b == 0u) return;
+        if (need) {
+            CoreEntry<T> e;
+            e.x = x;
+            e.y = y;
+            e.pref = pref;
+            e.dest = lane | (p << 5);
+            cq.q[qn + __popc(b & lt_mask)] = e;
+        }
+        qn += __popc(b);
+        __syncwarp();
+    };
 
     WorkItem w;
     while (next_item(a, P, lane, w)) {
         const size_t cbase = size_t(w.c) * size_t(a.n);
         const int* whi = a.whi + cbase;
         const int* wlo = a.wlo + cbase;
-        const int t0 = w.t0, t1 = w.t1;
+        const int* mi = a.mi;
+        const int kc = a.kc[w.c];
+        const int t0 = w.t0, t1 = w.t1, tl = t1 - 1;
         const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
         const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
+        const long fs = warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; });
+        const long Cb = warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; });
+        const long fe = Cb > fs ? Cb : fs;
+        const long E = warp_lower_bound(fs, fe, lane, [&](long i) { return mi[i] >= t0 - kc; });
+        const long Fc = warp_lower_bound(E, fe, lane, [&](long i) { return mi[i] > tl + kc; });
         const REC* recs = recs_all + cbase;
-        const AuxV64* aux = a.aux + cbase;
 
         int jj[P];
         float jf[P];
@@ -392,12 +606,197 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt(StepArgs a) {
         for (int p = 0; p < P; ++p) {
             jj[p] = t0 + lane + 32 * p;
             jf[p] = float(jj[p]);
-            const int jc = jj[p] < t1 ? jj[p] : t1 - 1;
-            fj[p] = MIXED ? 0.0 : F[jc];
+            fj[p] = MIXED ? 0.0 : F[jj[p] < t1 ? jj[p] : tl];
             accf[p] = sumf[p] = cmpf[p] = 0.0f;
             accd[p] = 0.0;
         }
-        const float t0f = float(t0), tlf = float(t1 - 1);
+
+        // Region I on every row: u = x^2 + Cy, acc += Pc (u + 1) / (u^2 + D2).
+        auto fast_line = [&](const REC& r) {
+            if (MIXED) {
+                const float4* q = reinterpret_cast<const float4*>(&r);
+                const float4 v0 = q[0], v1 = q[1];
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const float xs = fmaf(v0.x - jf[p], v0.z, v0.y);
+                    const float u = fmaf(xs, xs, v0.w);
+                    accf[p] = fmaf(fmaf(u, v1.y, v1.y), rcp_approx_f32(fmaf(u, u, v1.x)), accf[p]);
+                }
+            } else {
+                const double2* q = reinterpret_cast<const double2*>(&r);
+                const double2 v0 = q[0], v1 = q[1], v2 = q[2];
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const double xs = (v0.x - fj[p]) * v0.y;
+                    const double u = fma(xs, xs, v1.x);
+                    accd[p] = fma(fma(u, v2.x, v2.x), rcp_refined_f64(fma(u, u, v1.y)), accd[p]);
+                }
+            }
+        };
+        // `full`: the line's window covers the whole tile.
+        auto slow_line = [&](const REC& r, bool full) {
+            if (MIXED) {
+                const float4* q = reinterpret_cast<const float4*>(&r);
+                const float4 v0 = q[0], v1 = q[1], v2 = q[2];
+                const float m = v0.x, ra = v0.y, dfa = v0.z, Cy = v0.w;
+                const float D2 = v1.x, Pc = v1.y, pref = v1.z, y = v1.w;
+                const float lo = v2.x, hi = v2.y, clo = v2.z, chi = v2.w;
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const float r0 = float(t0 + 32 * p), r1 = r0 + 31.0f;
+                    if (!full && (r0 >= hi || r1 < lo)) continue;
+                    const bool row_in = full || (r0 >= lo && r1 < hi);
+                    const bool row_core = !(r1 < clo || r0 > chi);
+                    const float xs = fmaf(m - jf[p], dfa, ra);
+                    const float u = fmaf(xs, xs, Cy);
+                    const float v = fmaf(u, Pc, Pc) * rcp_approx_f32(fmaf(u, u, D2));
+                    if (row_in && !row_core) {
+                        accf[p] += v;
+                        continue;
+                    }
+                    const bool in = row_in || (jf[p] >= lo && jf[p] < hi);
+                    const float ax = fabsf(xs);
+                    const float sx = ax + y;
+                    const bool band = row_core && jf[p] >= clo && jf[p] <= chi;
+                    const bool r2 = in && band && sx < 15.0f && sx >= 5.5f;
+                    const bool deep = in && band && sx < 5.5f;
+                    float add = (in && !r2 && !deep) ? v : 0.0f;
+                    if (__any_sync(0xffffffffu, r2) && r2) add = pref * w4_region2_re<float>(ax, y);
+                    accf[p] += add;
+                    if (row_core) push(deep, ax, y, pref, p);
+                }
+            } else {
+                const double2* q = reinterpret_cast<const double2*>(&r);
+                const double2 v0 = q[0], v1 = q[1], v2 = q[2], v3 = q[3];
+                const int4 vi = reinterpret_cast<const int4*>(&r)[4];
+                const double nu = v0.x, g = v0.y, Cy = v1.x, D2 = v1.y, Pc = v2.x, y = v2.y;
+                const double pref = v3.x;
+                const int lo = vi.x, hi = vi.y, clo = vi.z, chi = vi.w;
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const int r0 = t0 + 32 * p, r1 = r0 + 31;
+                    if (!full && (r0 >= hi || r1 < lo)) continue;
+                    const bool row_in = full || (r0 >= lo && r1 < hi);
+                    const bool row_core = !(r1 < clo || r0 > chi);
+                    const double xs = (nu - fj[p]) * g;
+                    if (row_in && !row_core) {
+                        const double u = fma(xs, xs, Cy);
+                        accd[p] = fma(fma(u, Pc, Pc), rcp_refined_f64(fma(u, u, D2)), accd[p]);
+                        continue;
+                    }
+                    const bool in = row_in || (jj[p] >= lo && jj[p] < hi);
+                    // x and y are bit-identical to the reference's, so the
+                    // region choice below is the reference's.
+                    const double ax = fabs(xs);
+                    const bool exact = row_core && jj[p] >= clo && jj[p] <= chi && !(ax + y >= 15.0);
+                    if (in && !exact) {
+                        const double u = fma(xs, xs, Cy);
+                        accd[p] = fma(fma(u, Pc, Pc), rcp_refined_f64(fma(u, u, D2)), accd[p]);
+                    }
+                    if (row_core) push(in && exact, ax, y, pref, p);
+                }
+            }
+        };
+
+        // A line whose window covers only part of the tile and whose core
+        // band misses it: rows outside the window are skipped, the boundary
+        // row is masked lane by lane.
+        auto partial_line = [&](const REC& r) {
+            if (MIXED) {
+                const float4* q = reinterpret_cast<const float4*>(&r);
+                const float4 v0 = q[0], v1 = q[1], v2 = q[2];
+                const float lo = v2.x, hi = v2.y;
+                if (!(v2.w < float(t0) || v2.z > float(tl))) {
+                    slow_line(r, false);
+                    return;
+                }
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const float r0 = float(t0 + 32 * p), r1 = r0 + 31.0f;
+                    if (r0 >= hi || r1 < lo) continue;
+                    const float xs = fmaf(v0.x - jf[p], v0.z, v0.y);
+                    const float u = fmaf(xs, xs, v0.w);
+                    float rr = rcp_approx_f32(fmaf(u, u, v1.x));
+                    if (!(r0 >= lo && r1 < hi)) rr = (jf[p] >= lo && jf[p] < hi) ? rr : 0.0f;
+                    accf[p] = fmaf(fmaf(u, v1.y, v1.y), rr, accf[p]);
+                }
+            } else {
+                const double2* q = reinterpret_cast<const double2*>(&r);
+                const double2 v0 = q[0], v1 = q[1], v2 = q[2];
+                const int4 vi = reinterpret_cast<const int4*>(&r)[4];
+                const int lo = vi.x, hi = vi.y;
+                if (!(vi.w < t0 || vi.z > tl)) {
+                    slow_line(r, false);
+                    return;
+                }
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const int r0 = t0 + 32 * p, r1 = r0 + 31;
+                    if (r0 >= hi || r1 < lo) continue;
+                    const double xs = (v0.x - fj[p]) * v0.y;
+                    const double u = fma(xs, xs, v1.x);
+                    double rr = rcp_refined_f64(fma(u, u, v1.y));
+                    if (!(r0 >= lo && r1 < hi)) rr = (jj[p] >= lo && jj[p] < hi) ? rr : 0.0;
+                    accd[p] = fma(fma(u, v2.x, v2.x), rr, accd[p]);
+                }
+            }
+        };
+        // A line whose window covers the tile and whose core band may reach
+        // it: region I on every row except the band's pairs outside region
+        // I, which are queued.
+        auto core_line = [&](const REC& r) {
+            if (MIXED) {
+                const float4* q = reinterpret_cast<const float4*>(&r);
+                const float4 v0 = q[0], v1 = q[1], v2 = q[2];
+                const float clo = v2.z, chi = v2.w, y = v1.w;
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const float r0 = float(t0 + 32 * p), r1 = r0 + 31.0f;
+                    const float xs = fmaf(v0.x - jf[p], v0.z, v0.y);
+                    const float u = fmaf(xs, xs, v0.w);
+                    const float num = fmaf(u, v1.y, v1.y);
+                    const float rr = rcp_approx_f32(fmaf(u, u, v1.x));
+                    if (r1 < clo || r0 > chi) {
+                        accf[p] = fmaf(num, rr, accf[p]);
+                        continue;
+                    }
+                    // band row: region I as computed, region II in place,
+                    // regions III and IV through the queue
+                    const float ax = fabsf(xs);
+                    const float sx = ax + y;
+                    const bool band = jf[p] >= clo && jf[p] <= chi;
+                    const bool r2 = band && sx < 15.0f && sx >= 5.5f;
+                    const bool deep = band && sx < 5.5f;
+                    float add = (r2 || deep) ? 0.0f : num * rr;
+                    if (__any_sync(0xffffffffu, r2) && r2) add = v1.z * w4_region2_re<float>(ax, y);
+                    accf[p] += add;
+                    push(deep, ax, y, v1.z, p);
+                }
+            } else {
+                const double2* q = reinterpret_cast<const double2*>(&r);
+                const double2 v0 = q[0], v1 = q[1], v2 = q[2], v3 = q[3];
+                const int4 vi = reinterpret_cast<const int4*>(&r)[4];
+                const int clo = vi.z, chi = vi.w;
+                const double y = v2.y, pref = v3.x;
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const int r0 = t0 + 32 * p, r1 = r0 + 31;
+                    const double xs = (v0.x - fj[p]) * v0.y;
+                    if (r1 < clo || r0 > chi) {
+                        const double u = fma(xs, xs, v1.x);
+                        accd[p] = fma(fma(u, v2.x, v2.x), rcp_refined_f64(fma(u, u, v1.y)), accd[p]);
+                        continue;
+                    }
+                    const double ax = fabs(xs);
+                    const bool exact = jj[p] >= clo && jj[p] <= chi && !(ax + y >= 15.0);
+                    if (!exact) {
+                        const double u = fma(xs, xs, v1.x);
+                        accd[p] = fma(fma(u, v2.x, v2.x), rcp_refined_f64(fma(u, u, v1.y)), accd[p]);
+                    }
+                    push(exact, ax, y, pref, p);
+                }
+            }
+        };
 
         const long nl = Lb - La;
         const int ngroups = int((nl + 31) / 32);
@@ -417,84 +816,58 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt(StepArgs a) {
             }
             __syncwarp();
             const REC* R = buf + (gi & 1) * 32;
-            const long gbase = La + 32L * gi;
-            const int cnt = int(Lb - gbase < 32 ? Lb - gbase : 32);
-            for (int t = 0; t < cnt; ++t) {
-                if (MIXED) {
-                    const float4* q = reinterpret_cast<const float4*>(&R[t]);
-                    const float4 v0 = q[0], v1 = q[1], v2 = q[2];
-                    const float m = v0.x, ra = v0.y, dfa = v0.z, B = v0.w;
-                    const float A2 = v1.x, Pc = v1.y, Qc = v1.z, y = v1.w;
-                    const float lo = v2.x, hi = v2.y, clo = v2.z, chi = v2.w;
-                    const bool fast = (lo <= t0f) && (tlf < hi) && ((tlf < clo) || (t0f > chi));
-                    if (fast) {
-#pragma unroll
-                        for (int p = 0; p < P; ++p) {
-                            const float xs = fmaf(m - jf[p], dfa, ra);
-                            const float x2 = xs * xs;
-                            const float den = fmaf(x2, x2 + B, A2);
-                            const float num = fmaf(x2, Pc, Qc);
-                            accf[p] += __fdividef(num, den);
-                        }
-                    } else {
-#pragma unroll
-                        for (int p = 0; p < P; ++p) {
-                            if (jf[p] >= lo && jf[p] < hi) {
-                                const float xs = fmaf(m - jf[p], dfa, ra);
-                                const float ax = fabsf(xs);
-                                const bool r1 = (jf[p] < clo || jf[p] > chi) && (ax + y >= 15.0f) &&
-                                                (ax < 1.0e8f);
-                                if (r1) {
-                                    const float x2 = xs * xs;
-                                    const float den = fmaf(x2, x2 + B, A2);
-                                    const float num = fmaf(x2, Pc, Qc);
-                                    accf[p] += __fdividef(num, den);
-                                } else {
-                                    const AuxV64 ax64 = aux[gbase + t];
-                                    const double x = fabs(ax64.nu - F[jj[p]]) * ax64.g;
-                                    accf[p] += float(w4_re(x, ax64.y) * ax64.pref);
-                                }
-                            }
-                        }
-                    }
-                } else {
-                    const double2* q = reinterpret_cast<const double2*>(&R[t]);
-                    const double2 v0 = q[0], v1 = q[1], v2 = q[2];
-                    const int4 vi = reinterpret_cast<const int4*>(&R[t])[3];
-                    const double nu = v0.x, g = v0.y, B = v1.x, A2 = v1.y, Pc = v2.x, Qc = v2.y;
-                    const int lo = vi.x, hi = vi.y, clo = vi.z, chi = vi.w;
-                    const bool fast = (lo <= t0) && (t1 - 1 < hi) && ((t1 - 1 < clo) || (t0 > chi));
-                    if (fast) {
-#pragma unroll
-                        for (int p = 0; p < P; ++p) {
-                            const double xs = (nu - fj[p]) * g;
-                            const double x2 = xs * xs;
-                            const double den = fma(x2, x2 + B, A2);
-                            const double num = fma(x2, Pc, Qc);
-                            accd[p] += num / den;
-                        }
-                    } else {
-#pragma unroll
-                        for (int p = 0; p < P; ++p) {
-                            if (jj[p] >= lo && jj[p] < hi) {
-                                const AuxV64 ax64 = aux[gbase + t];
-                                const double x = fabs(nu - fj[p]) * g;
-                                accd[p] += w4_re(x, ax64.y) * ax64.pref;
-                            }
-                        }
-                    }
+            const long gb = La + 32L * gi;
+            const long ge = Lb - gb < 32 ? Lb : gb + 32;
+            auto lo_of = [&](long v) { return int((v < gb ? gb : (v > ge ? ge : v)) - gb); };
+            const int a0 = lo_of(La), a1 = lo_of(fs);
+            const int b1 = lo_of(E), c1 = lo_of(Fc), d1 = lo_of(fe), e1 = lo_of(Lb);
+            // slow lines of the three slow runs, one loop: t in [a0, a1) and
+            // [d1, e1) are partial, [b1, c1) cover the tile
+            for (int t = a0; t < e1; ++t) {
+                if (t == a1) t = b1;  // skip the first fast run
+                if (t == c1) t = d1;  // skip the second fast run
+                if (t >= e1) break;
+                if (t >= b1 && t < c1) core_line(R[t]);
+                else partial_line(R[t]);
+                while (qn >= 32) qn = core_queue_flush<P, MIXED>(cq, qn, 32, lane);
+            }
+            {
+                int t = a1;
+                for (; t + 1 < b1; t += 2) {
+                    fast_line(R[t]);
+                    fast_line(R[t + 1]);
                 }
+                if (t < b1) fast_line(R[t]);
+                t = c1;
+                for (; t + 1 < d1; t += 2) {
+                    fast_line(R[t]);
+                    fast_line(R[t + 1]);
+                }
+                if (t < d1) fast_line(R[t]);
             }
             if (MIXED) {
-                // Compensated (Kahan) fold of this group's FP32 partials.
+                // Pending core pairs, then the compensated (Kahan) fold of
+                // this group's FP32 partials.
+                if (qn > 0) qn = core_queue_flush<P, MIXED>(cq, qn, qn, lane);
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
-                    const float yk = accf[p] - cmpf[p];
+                    const float part = accf[p] + float(cq.corr[p][lane]);
+                    cq.corr[p][lane] = T(0);
+                    const float yk = part - cmpf[p];
                     const float tk = sumf[p] + yk;
                     cmpf[p] = (tk - sumf[p]) - yk;
                     sumf[p] = tk;
                     accf[p] = 0.0f;
                 }
+            }
+            __syncwarp();
+        }
+        if (!MIXED) {
+            while (qn > 0) qn = core_queue_flush<P, MIXED>(cq, qn, qn < 32 ? qn : 32, lane);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                accd[p] += double(cq.corr[p][lane]);
+                cq.corr[p][lane] = T(0);
             }
             __syncwarp();
         }
@@ -604,7 +977,12 @@ int blocks_per_sm(K kernel, int threads, size_t smem) {
 template <int P, int WARPS, bool MIXED>
 cudaError_t run_voigt(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
     using REC = typename std::conditional<MIXED, RecV32, RecV64>::type;
-    const size_t smem = size_t(WARPS) * 64 * sizeof(REC);
+    const size_t smem = size_t(WARPS) * (64 * sizeof(REC) + sizeof(WarpCoreQueue<P, MIXED>));
+    if (smem > 48 * 1024) {
+        if (cudaFuncSetAttribute(k_steptwo_voigt<P, WARPS, MIXED>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+            return cudaGetLastError();
+    }
     if (occ) {
         *occ = blocks_per_sm(k_steptwo_voigt<P, WARPS, MIXED>, WARPS * 32, smem);
         return cudaSuccess;
@@ -717,9 +1095,16 @@ size_t record_bytes(int kind, bool mixed) {
     return sizeof(RecE64);
 }
 
-size_t aux_bytes(int kind, bool mixed) {
-    (void)mixed;
-    return kind == kVoigt ? sizeof(AuxV64) : 0;
+ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off) {
+    auto al = [](size_t v) { return (v + 255) / 256 * 256; };
+    ScratchPlan p;
+    p.off_rec = al(base_off);
+    p.off_wlo = al(p.off_rec + record_bytes(kind, mixed) * n * size_t(ncond));
+    p.off_whi = al(p.off_wlo + sizeof(int) * n * size_t(ncond));
+    p.off_mi = al(p.off_whi + sizeof(int) * n * size_t(ncond));
+    p.off_kc = al(p.off_mi + sizeof(int) * n);
+    p.need = al(p.off_kc + sizeof(int) * size_t(kMaxCond));
+    return p;
 }
 
 }  // namespace xs

@@ -32,7 +32,7 @@ namespace {
 
 constexpr size_t kXsNoAllocScratchBytes = size_t(XS_NOALLOC_SCRATCH_BYTES);
 // First 256 bytes: [0] error bits, [1] work counter; the rest: records,
-// auxiliary data and windows, each section 256-byte aligned.
+// windows, line grid indices and core widths, each section 256-byte aligned.
 constexpr size_t kHeaderBytes = 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kXsNoAllocScratchBytes];
@@ -40,8 +40,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kXsNoAllocScrat
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 void* g_scratch_addr[kMaxDevices] = {};
-
-size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 int noalloc_fail(int code, const char* msg) { return xs::set_error(code, msg); }
 
@@ -80,14 +78,10 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
 
     // Size check against the fixed array, before touching the device.
     const size_t nl = size_t(n > 0 ? n : 0);
-    const size_t rb = xs::record_bytes(kind, mixed), ab = xs::aux_bytes(kind, mixed);
-    const size_t off_rec = kHeaderBytes;
-    const size_t off_aux = align_up(off_rec + rb * nl, 256);
-    const size_t off_wlo = align_up(off_aux + ab * nl, 256);
-    const size_t off_whi = align_up(off_wlo + sizeof(int) * nl, 256);
-    const size_t need = align_up(off_whi + sizeof(int) * nl, 256);
+    const xs::ScratchPlan plan = xs::plan_scratch(kind, mixed, nl, 1, kHeaderBytes);
+    const size_t need = plan.need;
     if (need > kXsNoAllocScratchBytes) {
-        const size_t per = rb + ab + 2 * sizeof(int);
+        const size_t per = xs::record_bytes(kind, mixed) + 3 * sizeof(int);
         char msg[256];
         std::snprintf(msg, sizeof(msg),
                       "xs_execute_noalloc: %zu lines need %zu scratch bytes; the fixed array holds "
@@ -156,10 +150,11 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
     pa.G = G;
     pa.ncond = 1;
     pa.cond[0] = xs::make_cond(*opt, *cond);
-    pa.rec = base + off_rec;
-    pa.aux = ab ? base + off_aux : nullptr;
-    pa.wlo = reinterpret_cast<int*>(base + off_wlo);
-    pa.whi = reinterpret_cast<int*>(base + off_whi);
+    pa.rec = base + plan.off_rec;
+    pa.wlo = reinterpret_cast<int*>(base + plan.off_wlo);
+    pa.whi = reinterpret_cast<int*>(base + plan.off_whi);
+    pa.mi = reinterpret_cast<int*>(base + plan.off_mi);
+    pa.kc = reinterpret_cast<int*>(base + plan.off_kc);
     pa.err = words;
     pa.half_width = opt->half_width;
     pa.x0 = opt->dfreq * 0.5;
@@ -172,9 +167,10 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
     xs::StepArgs sa;
     std::memset(&sa, 0, sizeof(sa));
     sa.rec = pa.rec;
-    sa.aux = static_cast<const xs::AuxV64*>(pa.aux);
     sa.wlo = pa.wlo;
     sa.whi = pa.whi;
+    sa.mi = pa.mi;
+    sa.kc = pa.kc;
     sa.n = n;
     sa.out = out;
     sa.out_stride = 0;
@@ -194,9 +190,11 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
     const long want = (long(sa.n_items) + W - 1) / W;
     const int blocks = int(want < long(occ) * sms ? want : long(occ) * sms);
 
-    // The array keeps the previous call's contents: the error word and the
-    // work counter must start at zero; records and windows are rewritten.
+    // The array keeps the previous call's contents: the error word, the
+    // work counter and the core widths must start at zero; records, windows
+    // and grid indices are rewritten.
     cudaError_t e = cudaMemsetAsync(words, 0, 2 * sizeof(unsigned), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(xs::kMaxCond), st);
     if (e == cudaSuccess) e = xs::launch_grid_check(G, words, st);
     if (e == cudaSuccess) e = xs::launch_prep(kind, opt->convention, mixed, pa, st);
     if (e == cudaSuccess) e = xs::launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);
