@@ -48,14 +48,15 @@ def log(*a):
 # --------------------------------------------------------------------------
 # workload
 # --------------------------------------------------------------------------
-def sweep_workload(n_lines: int, grid_points: int, rank: int = 0, workload: str = "sweep"):
+def sweep_workload(n_lines: int, grid_points: int, rank: int = 0, workload: str = "sweep",
+                   pbar: float = 1.0):
     from gpu_cross_b200 import synth
 
     if workload == "single":
         # Voigt single point: T = 1000 K, P = 1 bar, grid 500-8000 at 0.01
         lines, grid, cond = synth.voigt_single_workload(n_lines, grid_points)
         conds = [dict(temperature=cond["temperature"], partition=cond["partition"],
-                      pressure_atm=1.0, cut=25.0)]
+                      pressure_atm=pbar, cut=25.0)]
         common = dict(mean_mass=cond["mean_mass"], ref_temp=cond["ref_temp"])
     else:
         lines, grid, conds, common = synth.voigt_sweep_workload(n_lines, grid_points)
@@ -187,6 +188,29 @@ def reference_cpu_sample(lines, grid, cond, common, target_s: float = 12.0, thre
     return rate, threads, desc
 
 
+def reference_gpu_sample(lines, grid, cond, common, n_lines: int = 400_000):
+    """Time the reference's own step-one/step-two kernels (cross_kernal.cu for
+    sm_100a, oracle/_ref/libref_gpu.so) on a contiguous slice of the list for
+    one condition, chunked at 80000 grid points as BaseProfile does."""
+    import oracle
+
+    fr = grid.freq()
+    mid = len(lines) // 2
+    part = lines.slice(mid - n_lines // 2, mid + n_lines // 2)
+    part.gamma = part.gamma * cond["pressure_atm"]
+    c = dict(temperature=cond["temperature"], partition=cond["partition"],
+             mean_mass=common["mean_mass"], pressure=1.0, ref_temp=common["ref_temp"])
+    span_pts = (part.nu[-1] - part.nu[0]) / grid.dfreq + 2 * 25.0 / grid.dfreq
+    chunks = max(1, int(np.ceil(span_pts / 80000.0)))
+    z = np.zeros_like(fr)
+    _, ms = oracle.ref_gpu(oracle.VOIGT, fr, z, part, c, grid.dfreq, chunks=chunks)
+    pairs = pairs_gpu_window(part.nu, fr, 25.0)
+    return {"value": pairs / (ms * 1e-3), "unit": "line-evals/s", "kernel_ms": ms,
+            "sample": f"reference cross_kernal.cu (FP64, sm_100a) step one + step two, one condition "
+                      f"(T={cond['temperature']:.0f} K), {len(part)} lines nu {part.nu[0]:.1f}-"
+                      f"{part.nu[-1]:.1f} cm-1, {chunks} chunk(s), {pairs:.3e} pairs"}
+
+
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
@@ -197,7 +221,8 @@ def run_ours(args, rank, world, dist):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    lines, grid, conds, common = sweep_workload(args.lines, args.points, rank, args.workload)
+    lines, grid, conds, common = sweep_workload(args.lines, args.points, rank, args.workload,
+                                                args.pbar)
     if args.conds < len(conds):
         step = len(conds) / float(args.conds)
         conds = [conds[int(k * step)] for k in range(args.conds)]
@@ -225,9 +250,9 @@ def run_ours(args, rank, world, dist):
     G = capi.make_grid(dfr)
     o_mix = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.MIXED,
                               ref_temp=common["ref_temp"], points_per_thread=args.P,
-                              warps_per_block=args.W)
+                              warps_per_block=args.W, conditions_per_warp=args.C)
     o_f64 = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.FP64,
-                              ref_temp=common["ref_temp"])
+                              ref_temp=common["ref_temp"], conditions_per_warp=args.C64)
     g_mix = eng.capture(o_mix, cc, L, G, out.data_ptr(), npts, zero_out=True)
     eng2 = g_f64 = None
     if not args.no_fp64:
@@ -342,6 +367,16 @@ def run_ours(args, rank, world, dist):
         except (OSError, ValueError):
             traffic = None
 
+    # the reference's own GPU kernels (cross_kernal.cu built for sm_100a) on a
+    # bounded sample: one condition, a nu-slice of the list, chunked the way
+    # BaseProfile feeds GpuManager (MAX-POINTS 80000 per chunk)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        try:
+            ref_gpu = reference_gpu_sample(lines, grid, conds[min(26, len(conds) - 1)], common)
+        except Exception as exc:
+            ref_gpu = {"value": None, "sample": f"not run: {exc}"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -376,14 +411,18 @@ def run_ours(args, rank, world, dist):
         "dtype": "f32 profile / f64 offsets+intensities+tile sums",
         "data": "synthetic (seeded; no line list ships with the reference)",
         "config": {
-            "workload": "voigt_sweep_40tp: 1e7 lines, nu U(500,8000), grid 500-8000 cm-1 at 0.1 "
-                        "(7.5e4 points), T 300-2100 K x P {1e-3,0.1,1,10} bar, cut 25 cm-1, "
-                        "mixed precision, one CUDA-graph replay per step",
+            "workload": (("voigt_sweep_40tp: 1e7 lines, nu U(500,8000), grid 500-8000 cm-1 at 0.1 "
+                          "(7.5e4 points), T 300-2100 K x P {1e-3,0.1,1,10} bar, cut 25 cm-1")
+                         if args.workload == "sweep" else
+                         ("voigt_single: 1e7 lines, nu U(500,8000), grid 500-8000 cm-1 at 0.01 "
+                          "(7.5e5 points), T 1000 K, P 1 bar, cut 25 cm-1"))
+                        + ", mixed precision, one CUDA-graph replay per step",
             "lines": len(lines), "grid_points": npts, "conditions": nc,
             "line_evals_per_step": pairs_step,
             "parallelism": f"{world} rank(s), independent (T,P) batches, no collective",
-            "l2": "inputs larger than L2 (records ~19 GB per step), no flush",
+            "l2": "inputs larger than L2 (per-step records > 0.6 GB), no flush",
             "points_per_thread": args.P or 4, "warps_per_block": args.W or 8,
+            "conditions_per_warp": args.C or "auto",
         },
         "accuracy_vs_fp64": {"max_rel_above_1e-6_peak": rel_max, "max_integrated_rel": integ_max},
         "fp64": {"value": f64_value, "ms_per_step": f64_step, "unit": "line-evals/s"},
@@ -397,6 +436,7 @@ def run_ours(args, rank, world, dist):
             "other_peaks": peaks,
         },
         "cpu_baseline": cpu,
+        "reference_gpu_kernel": ref_gpu,
         "e2e": {"value": e2e_value, "unit": "line-evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": 3 * args.steps,
@@ -454,11 +494,16 @@ def main():
     ap.add_argument("--lines", type=int, default=10_000_000)
     ap.add_argument("--points", type=int, default=0, help="grid points (default per workload)")
     ap.add_argument("--workload", choices=["sweep", "single"], default="sweep")
+    ap.add_argument("--pbar", type=float, default=1.0,
+                    help="single workload: pressure factor on the 1-bar Lorentz widths")
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--W", type=int, default=0)
+    ap.add_argument("--C", type=int, default=0, help="conditions per warp (mixed)")
+    ap.add_argument("--C64", type=int, default=0, help="conditions per warp (FP64)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--conds", type=int, default=40, help="subset of the 40 conditions (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()

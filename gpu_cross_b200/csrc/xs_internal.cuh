@@ -84,6 +84,35 @@ struct __align__(16) RecV32 {
 };
 static_assert(sizeof(RecV32) == 64, "RecV32 layout");
 
+// Multi-condition layout: a group of C conditions that share one window
+// (same cut) is evaluated together, one 32-point row of the grid per warp
+// and C accumulators per lane.  What the conditions share is stored once per
+// line; the rest once per (line, condition), conditions innermost.
+// core packs the core band around m: (m - clo) | (chi - m) << 16, each part
+// at most 0x7fff (0x7fff: unbounded); -1: no core band.
+struct __align__(16) LineSh32 {
+    float m;
+    int lo, hi;
+    int pad;
+};
+static_assert(sizeof(LineSh32) == 16, "LineSh32 layout");
+struct __align__(16) CondRec32 {
+    float ra, dfa, Cy, D2;
+    float Pc, pref, y;
+    int core;
+};
+static_assert(sizeof(CondRec32) == 32, "CondRec32 layout");
+struct __align__(16) LineSh64 {
+    double nu;
+    int lo, hi;
+};
+static_assert(sizeof(LineSh64) == 16, "LineSh64 layout");
+struct __align__(16) CondRec64 {
+    double g, Cy, D2, Pc, y, pref;
+    int core, pad0, pad1, pad2;
+};
+static_assert(sizeof(CondRec64) == 64, "CondRec64 layout");
+
 // Doppler / Gaussian record (FP64).
 struct __align__(16) RecE64 {
     double nu;  // centre used for offsets
@@ -123,6 +152,9 @@ struct PrepArgs {
     double x0;          // Doppler half bin: dfreq * 0.5
     double xg, x0g;     // Gaussian: sqrt(ln2)/HW, xg * dfreq * 0.5
     int mixed_tile_span;  // 32 * points_per_thread (mixed safety bound)
+    int group;          // > 0: multi-condition layout with this many
+                        // conditions per group (Voigt only)
+    void* lsh;          // multi-condition: per-line shared records per group
 };
 
 struct StepArgs {
@@ -135,6 +167,8 @@ struct StepArgs {
     double* out;
     size_t out_stride;  // elements between conditions
     GridDev G;
+    const void* lsh;    // multi-condition layout (see LineSh32)
+    int group;          // conditions per group (multi-condition kernel)
     int tiles_per_cond;
     int n_items;
     unsigned* counter;
@@ -155,8 +189,14 @@ size_t record_bytes(int kind, bool mixed);
 // `ncond` conditions of `n` lines, the per-line grid index and the
 // per-condition core widths; sections 256-byte aligned from `base_off`.
 struct ScratchPlan {
-    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, need;
+    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, need;
 };
-ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off);
+ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off,
+                         int group = 0);
+
+// Multi-condition step two (Voigt): C conditions per warp, 32 points per warp.
+cudaError_t launch_steptwo_mc(bool mixed, int C, int warps, int blocks, const StepArgs& a,
+                              cudaStream_t stream);
+int steptwo_mc_blocks_per_sm(bool mixed, int C, int warps);
 
 }  // namespace xs

@@ -27,6 +27,9 @@
 namespace xs {
 namespace {
 
+// Depth of the per-warp cp.async staging pipeline (groups of 32 records).
+constexpr int kStages = 3;
+
 // ---------------------------------------------------------------------------
 // Small complex arithmetic for the W4 regions II-IV.
 // ---------------------------------------------------------------------------
@@ -229,6 +232,63 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c) {
             kcl = w < 3.0e7 ? int(w) : 30000000;
         }
         if (c == 0) a.mi[i] = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
+        if (a.group > 0) {
+            // Multi-condition layout (conditions of a group share the window).
+            const int C = a.group;
+            const int cg = c / C, cl = c - cg * C;
+            const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(i);
+            int core = -1;
+            if (whole) {
+                core = 0x7fff | (0x7fff << 16);
+            } else if (chi_d >= clo_d) {
+                const int aa = int(fmin(m - clo_d, 32767.0));
+                const int bb = int(fmin(chi_d - m, 32767.0));
+                core = aa | (bb << 16);
+            }
+            if (MIXED) {
+                CondRec32 cr;
+                cr.ra = float(((nu_p - f0) - m * df) * g);
+                cr.dfa = float(df * g);
+                cr.Cy = float(Cy);
+                cr.D2 = float(D2);
+                cr.Pc = float(Pc);
+                cr.pref = float(pref);
+                cr.y = float(y);
+                cr.core = core;
+                reinterpret_cast<CondRec32*>(a.rec)[gi * C + cl] = cr;
+                if (cl == 0) {
+                    LineSh32 ls;
+                    ls.m = float(fabs(m) < 16000000.0 ? m : 0.0);
+                    ls.lo = lo;
+                    ls.hi = hi;
+                    ls.pad = 0;
+                    reinterpret_cast<LineSh32*>(a.lsh)[gi] = ls;
+                }
+            } else {
+                CondRec64 cr;
+                cr.g = g;
+                cr.Cy = Cy;
+                cr.D2 = D2;
+                cr.Pc = Pc;
+                cr.y = y;
+                cr.pref = pref;
+                cr.core = core;
+                cr.pad0 = cr.pad1 = cr.pad2 = 0;
+                reinterpret_cast<CondRec64*>(a.rec)[gi * C + cl] = cr;
+                if (cl == 0) {
+                    LineSh64 ls;
+                    ls.nu = nu_p;
+                    ls.lo = lo;
+                    ls.hi = hi;
+                    reinterpret_cast<LineSh64*>(a.lsh)[gi] = ls;
+                }
+            }
+            if (cl == 0) {
+                a.wlo[gi] = lo;
+                a.whi[gi] = hi;
+            }
+            return kcl;
+        }
         if (MIXED) {
             RecV32 rr;
             rr.m = float(fabs(m) < 16000000.0 ? m : 0.0);
@@ -356,18 +416,15 @@ __device__ long warp_lower_bound(long lo, long hi, int lane, Pred pred) {
     return r < hi ? r : hi;
 }
 
-// Copy `cnt` records of REC (sizeof a multiple of 16) into shared memory.
+// Copy `cnt` records of REC (sizeof a multiple of 16) into shared memory,
+// 16 bytes per lane per step.
 template <class REC>
 __device__ __forceinline__ void stage(REC* dst, const REC* src, int cnt, int lane) {
     constexpr int kChunks = sizeof(REC) / 16;
     const int total = cnt * kChunks;
     const char* s = reinterpret_cast<const char*>(src);
     char* d = reinterpret_cast<char*>(dst);
-#pragma unroll
-    for (int k = 0; k < kChunks; ++k) {
-        const int q = lane + 32 * k;
-        if (q < total) cp_async16(d + 16 * q, s + 16 * q);
-    }
+    for (int q = lane; q < total; q += 32) cp_async16(d + 16 * q, s + 16 * q);
 }
 
 struct WorkItem {
@@ -555,8 +612,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    REC* buf = reinterpret_cast<REC*>(smem_raw) + warp * 64;
-    Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 64 * sizeof(REC))[warp];
+    REC* buf = reinterpret_cast<REC*>(smem_raw) + warp * 32 * kStages;
+    Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 32 * kStages * sizeof(REC))[warp];
     const REC* recs_all = reinterpret_cast<const REC*>(a.rec);
     const double* F = a.G.freq;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -800,22 +857,24 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
 
         const long nl = Lb - La;
         const int ngroups = int((nl + 31) / 32);
-        if (ngroups > 0) {
-            stage(buf, recs + La, int(nl < 32 ? nl : 32), lane);
-            cp_async_commit();
-        }
-        for (int gi = 0; gi < ngroups; ++gi) {
-            if (gi + 1 < ngroups) {
-                const long b = La + 32L * (gi + 1);
+        // kStages-deep cp.async pipeline: groups gi+1 .. gi+kStages-1 are in
+        // flight while group gi is evaluated (one commit per step, empty
+        // commits past the end keep the group count uniform).
+        auto issue = [&](int g) {
+            if (g < ngroups) {
+                const long b = La + 32L * g;
                 const long rem = Lb - b;
-                stage(buf + ((gi + 1) & 1) * 32, recs + b, int(rem < 32 ? rem : 32), lane);
-                cp_async_commit();
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
+                stage(buf + (g % kStages) * 32, recs + b, int(rem < 32 ? rem : 32), lane);
             }
+            cp_async_commit();
+        };
+#pragma unroll
+        for (int g = 0; g < kStages - 1; ++g) issue(g);
+        for (int gi = 0; gi < ngroups; ++gi) {
+            issue(gi + kStages - 1);
+            cp_async_wait<kStages - 1>();
             __syncwarp();
-            const REC* R = buf + (gi & 1) * 32;
+            const REC* R = buf + (gi % kStages) * 32;
             const long gb = La + 32L * gi;
             const long ge = Lb - gb < 32 ? Lb : gb + 32;
             auto lo_of = [&](long v) { return int((v < gb ? gb : (v > ge ? ge : v)) - gb); };
@@ -862,6 +921,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             }
             __syncwarp();
         }
+        cp_async_wait<0>();
+        __syncwarp();
         if (!MIXED) {
             while (qn > 0) qn = core_queue_flush<P, MIXED>(cq, qn, qn < 32 ? qn : 32, lane);
 #pragma unroll
@@ -877,6 +938,224 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             if (jj[p] < t1) {
                 const double v = MIXED ? double(sumf[p]) - double(cmpf[p]) : accd[p];
                 out[jj[p]] += v;
+            }
+        }
+    }
+}
+
+// Multi-condition step two: a work item is (group of C conditions that share
+// one window, row of 32 grid points); each lane owns one grid point and C
+// accumulators.  The line runs are found as in k_steptwo_voigt (windows and
+// grid indices are shared by the group; the core run uses the group's widest
+// core), and every line loads its shared record once and one small record
+// per condition.
+template <int C, int WARPS, bool MIXED>
+constexpr int voigt_mc_min_blocks() {
+    return MIXED ? 24 / WARPS : 1;
+}
+
+template <int C, int WARPS, bool MIXED>
+__global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIXED>()))
+    k_steptwo_voigt_mc(StepArgs a) {
+    using CR = typename std::conditional<MIXED, CondRec32, CondRec64>::type;
+    using LS = typename std::conditional<MIXED, LineSh32, LineSh64>::type;
+    using T = typename std::conditional<MIXED, float, double>::type;
+    using Q = WarpCoreQueue<C, MIXED>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    LS* lsb = reinterpret_cast<LS*>(smem_raw) + warp * 64;
+    CR* crb = reinterpret_cast<CR*>(smem_raw + size_t(WARPS) * 64 * sizeof(LS)) + warp * 64 * C;
+    Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 64 * (sizeof(LS) + C * sizeof(CR)))[warp];
+    const double* F = a.G.freq;
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+#pragma unroll
+    for (int c = 0; c < C; ++c) cq.corr[c][lane] = T(0);
+    int qn = 0;
+    auto push = [&](bool need, T x, T y, T pref, int c) {
+        const unsigned b = __ballot_sync(0xffffffffu, need);
+        if (b == 0u) return;
+        if (need) {
+            CoreEntry<T> e;
+            e.x = x;
+            e.y = y;
+            e.pref = pref;
+            e.dest = lane | (c << 5);
+            cq.q[qn + __popc(b & lt_mask)] = e;
+        }
+        qn += __popc(b);
+        __syncwarp();
+    };
+
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = int(atomicAdd(a.counter, 1u));
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.n_items) break;
+        const int cg = item / a.tiles_per_cond;
+        const int tile = item - cg * a.tiles_per_cond;
+        const int t0 = a.G.start + tile * 32;
+        const int end = a.G.start + a.G.points;
+        const int t1 = t0 + 32 < end ? t0 + 32 : end;
+        const int tl = t1 - 1;
+        const size_t gbase = size_t(cg) * size_t(a.n);
+        const int* whi = a.whi + gbase;
+        const int* wlo = a.wlo + gbase;
+        const int* mi = a.mi;
+        int kc = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) kc = max(kc, a.kc[cg * C + c]);
+        const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
+        const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
+        const long fs = warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; });
+        const long Cb = warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; });
+        const long fe = Cb > fs ? Cb : fs;
+        const long E = warp_lower_bound(fs, fe, lane, [&](long i) { return mi[i] >= t0 - kc; });
+        const long Fc = warp_lower_bound(E, fe, lane, [&](long i) { return mi[i] > tl + kc; });
+        const LS* lsh = reinterpret_cast<const LS*>(a.lsh) + gbase;
+        const CR* crec = reinterpret_cast<const CR*>(a.rec) + gbase * C;
+
+        const int jj = t0 + lane;
+        const float jf = float(jj);
+        const double fj = MIXED ? 0.0 : F[jj < t1 ? jj : tl];
+        float accf[C], sumf[C], cmpf[C];
+        double accd[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            accf[c] = sumf[c] = cmpf[c] = 0.0f;
+            accd[c] = 0.0;
+        }
+
+        // x (in Doppler widths) of this lane's point for condition record r.
+        auto offset = [&](const LS& s, const CR& r) -> T {
+            if constexpr (MIXED) return T(fmaf(float(s.m) - jf, float(r.dfa), float(r.ra)));
+            else return T((double(s.nu) - fj) * double(r.g));
+        };
+        auto region1 = [&](T xs, const CR& r, T mask, int c) {
+            if (MIXED) {
+                const float u = fmaf(float(xs), float(xs), float(r.Cy));
+                accf[c] = fmaf(fmaf(u, float(r.Pc), float(r.Pc)),
+                               rcp_approx_f32(fmaf(u, u, float(r.D2))) * float(mask), accf[c]);
+            } else {
+                const double u = fma(double(xs), double(xs), double(r.Cy));
+                accd[c] = fma(fma(u, double(r.Pc), double(r.Pc)),
+                              rcp_refined_f64(fma(u, u, double(r.D2))) * double(mask), accd[c]);
+            }
+        };
+        // One condition of a partial line, or of a line whose core band may
+        // reach this row; `in`: this lane's point lies in the line's window.
+        auto core_cond = [&](const LS& s, const CR& r, int mline, bool in, int c) {
+            const T xs = offset(s, r);
+            const T ax = xs < T(0) ? -xs : xs;
+            const T sx = ax + T(r.y);
+            bool band = false;
+            if (r.core != -1) {
+                const int aa = r.core & 0xffff, bb = (r.core >> 16) & 0xffff;
+                const int rel = jj - mline;
+                band = (aa == 0x7fff || rel >= -aa) && (bb == 0x7fff || rel <= bb);
+            }
+            // x and y of the FP64 path are bit-identical to the reference's,
+            // so |x| + y < 15 is the reference's region choice there.
+            const bool special = in && band && sx < T(15);
+            if (!__any_sync(0xffffffffu, special)) {
+                region1(xs, r, in ? T(1) : T(0), c);
+                return;
+            }
+            const bool r2 = MIXED && special && sx >= T(5.5);
+            const bool deep = special && !r2;
+            region1(xs, r, (in && !special) ? T(1) : T(0), c);
+            if (MIXED) {
+                if (__any_sync(0xffffffffu, r2) && r2)
+                    accf[c] += float(r.pref) * w4_region2_re<float>(float(ax), float(r.y));
+            }
+            push(deep, ax, T(r.y), T(r.pref), c);
+        };
+
+        const long nl = Lb - La;
+        const int ngroups = int((nl + 31) / 32);
+        auto stage_group = [&](int bufi, long b, int cnt) {
+            stage(lsb + bufi * 32, lsh + b, cnt, lane);
+            stage(crb + bufi * 32 * C, crec + b * C, cnt * C, lane);
+        };
+        if (ngroups > 0) {
+            stage_group(0, La, int(nl < 32 ? nl : 32));
+            cp_async_commit();
+        }
+        for (int gi = 0; gi < ngroups; ++gi) {
+            if (gi + 1 < ngroups) {
+                const long b = La + 32L * (gi + 1);
+                const long rem = Lb - b;
+                stage_group((gi + 1) & 1, b, int(rem < 32 ? rem : 32));
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncwarp();
+            const LS* SL = lsb + (gi & 1) * 32;
+            const CR* SC = crb + (gi & 1) * 32 * C;
+            const long gb = La + 32L * gi;
+            const long ge = Lb - gb < 32 ? Lb : gb + 32;
+            auto lo_of = [&](long v) { return int((v < gb ? gb : (v > ge ? ge : v)) - gb); };
+            const int a0 = lo_of(La), a1 = lo_of(fs), b1 = lo_of(E), c1 = lo_of(Fc), d1 = lo_of(fe),
+                      e1 = lo_of(Lb);
+            // fast lines: window covers the row, no core near it
+            {
+                int t = a1;
+                for (; t < b1; ++t) {
+                    const LS s = SL[t];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], T(1), c);
+                }
+                for (t = c1; t < d1; ++t) {
+                    const LS s = SL[t];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], T(1), c);
+                }
+            }
+            // core lines (window covers the row) and partial lines
+            for (int t = a0; t < e1; ++t) {
+                if (t == a1) t = b1;
+                if (t == c1) t = d1;
+                if (t >= e1) break;
+                const LS s = SL[t];
+                const bool full = (t >= b1 && t < c1);
+                const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
+                const int mline = mi[gb + t];
+#pragma unroll
+                for (int c = 0; c < C; ++c) core_cond(s, SC[t * C + c], mline, in, c);
+                while (qn >= 32) qn = core_queue_flush<C, MIXED>(cq, qn, 32, lane);
+            }
+            if (MIXED) {
+                if (qn > 0) qn = core_queue_flush<C, MIXED>(cq, qn, qn, lane);
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const float part = accf[c] + float(cq.corr[c][lane]);
+                    cq.corr[c][lane] = T(0);
+                    const float yk = part - cmpf[c];
+                    const float tk = sumf[c] + yk;
+                    cmpf[c] = (tk - sumf[c]) - yk;
+                    sumf[c] = tk;
+                    accf[c] = 0.0f;
+                }
+            }
+            __syncwarp();
+        }
+        if (!MIXED) {
+            while (qn > 0) qn = core_queue_flush<C, MIXED>(cq, qn, qn < 32 ? qn : 32, lane);
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                accd[c] += double(cq.corr[c][lane]);
+                cq.corr[c][lane] = T(0);
+            }
+            __syncwarp();
+        }
+        if (jj < t1) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const double v = MIXED ? double(sumf[c]) - double(cmpf[c]) : accd[c];
+                a.out[size_t(cg * C + c) * a.out_stride + size_t(jj)] += v;
             }
         }
     }
@@ -977,7 +1256,7 @@ int blocks_per_sm(K kernel, int threads, size_t smem) {
 template <int P, int WARPS, bool MIXED>
 cudaError_t run_voigt(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
     using REC = typename std::conditional<MIXED, RecV32, RecV64>::type;
-    const size_t smem = size_t(WARPS) * (64 * sizeof(REC) + sizeof(WarpCoreQueue<P, MIXED>));
+    const size_t smem = size_t(WARPS) * (32 * kStages * sizeof(REC) + sizeof(WarpCoreQueue<P, MIXED>));
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(k_steptwo_voigt<P, WARPS, MIXED>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
@@ -989,6 +1268,43 @@ cudaError_t run_voigt(int blocks, const StepArgs& a, cudaStream_t st, int* occ) 
     }
     k_steptwo_voigt<P, WARPS, MIXED><<<blocks, WARPS * 32, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+template <int C, int WARPS, bool MIXED>
+cudaError_t run_voigt_mc(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
+    using CR = typename std::conditional<MIXED, CondRec32, CondRec64>::type;
+    using LS = typename std::conditional<MIXED, LineSh32, LineSh64>::type;
+    const size_t smem = size_t(WARPS) * (64 * (sizeof(LS) + C * sizeof(CR)) + sizeof(WarpCoreQueue<C, MIXED>));
+    if (smem > 48 * 1024) {
+        if (cudaFuncSetAttribute(k_steptwo_voigt_mc<C, WARPS, MIXED>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+            return cudaGetLastError();
+    }
+    if (occ) {
+        *occ = blocks_per_sm(k_steptwo_voigt_mc<C, WARPS, MIXED>, WARPS * 32, smem);
+        return cudaSuccess;
+    }
+    k_steptwo_voigt_mc<C, WARPS, MIXED><<<blocks, WARPS * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int WARPS, bool MIXED>
+cudaError_t dispatch_mc_c(int C, int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
+    switch (C) {
+        case 2: return run_voigt_mc<2, WARPS, MIXED>(blocks, a, st, occ);
+        case 4: return run_voigt_mc<4, WARPS, MIXED>(blocks, a, st, occ);
+        case 8: return run_voigt_mc<8, WARPS, MIXED>(blocks, a, st, occ);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t dispatch_mc(bool mixed, int C, int warps, int blocks, const StepArgs& a,
+                        cudaStream_t st, int* occ) {
+    if (warps == 4) return mixed ? dispatch_mc_c<4, true>(C, blocks, a, st, occ)
+                                 : dispatch_mc_c<4, false>(C, blocks, a, st, occ);
+    if (warps == 8) return mixed ? dispatch_mc_c<8, true>(C, blocks, a, st, occ)
+                                 : dispatch_mc_c<8, false>(C, blocks, a, st, occ);
+    return cudaErrorInvalidValue;
 }
 
 template <int KIND, int CONV, int P, int WARPS>
@@ -1090,20 +1406,37 @@ int steptwo_blocks_per_sm(int kind, int conv, bool mixed, int P, int warps) {
     return occ;
 }
 
+cudaError_t launch_steptwo_mc(bool mixed, int C, int warps, int blocks, const StepArgs& a,
+                              cudaStream_t stream) {
+    if (blocks <= 0 || a.n_items <= 0) return cudaSuccess;
+    return dispatch_mc(mixed, C, warps, blocks, a, stream, nullptr);
+}
+
+int steptwo_mc_blocks_per_sm(bool mixed, int C, int warps) {
+    StepArgs dummy{};
+    int occ = 0;
+    if (dispatch_mc(mixed, C, warps, 0, dummy, nullptr, &occ) != cudaSuccess) return 0;
+    return occ;
+}
+
 size_t record_bytes(int kind, bool mixed) {
     if (kind == kVoigt) return mixed ? sizeof(RecV32) : sizeof(RecV64);
     return sizeof(RecE64);
 }
 
-ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off) {
+ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off, int group) {
     auto al = [](size_t v) { return (v + 255) / 256 * 256; };
     ScratchPlan p;
+    const size_t rec = group > 0 ? (mixed ? sizeof(CondRec32) : sizeof(CondRec64))
+                                 : record_bytes(kind, mixed);
+    const size_t nwin = group > 0 ? size_t((ncond + group - 1) / group) : size_t(ncond);
     p.off_rec = al(base_off);
-    p.off_wlo = al(p.off_rec + record_bytes(kind, mixed) * n * size_t(ncond));
-    p.off_whi = al(p.off_wlo + sizeof(int) * n * size_t(ncond));
-    p.off_mi = al(p.off_whi + sizeof(int) * n * size_t(ncond));
+    p.off_wlo = al(p.off_rec + rec * n * size_t(ncond));
+    p.off_whi = al(p.off_wlo + sizeof(int) * n * nwin);
+    p.off_mi = al(p.off_whi + sizeof(int) * n * nwin);
     p.off_kc = al(p.off_mi + sizeof(int) * n);
-    p.need = al(p.off_kc + sizeof(int) * size_t(kMaxCond));
+    p.off_lsh = al(p.off_kc + sizeof(int) * size_t(kMaxCond));
+    p.need = al(p.off_lsh + (group > 0 ? sizeof(LineSh32) * n * nwin : 0));
     return p;
 }
 

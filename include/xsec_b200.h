@@ -103,6 +103,9 @@ typedef struct {
     double dfreq;     /* grid step (the reference's cross_constants.dfreq) */
     int points_per_thread; /* 0 = autotuned; else 1, 2, 4 or 8 */
     int warps_per_block;   /* 0 = autotuned; else 4 or 8 */
+    int conditions_per_warp; /* VOIGT batches: 0 = automatic, 1 = one condition
+                                per warp, 2/4/8 = that many conditions with the
+                                same cut evaluated together by each warp */
 } xs_options;
 
 /* Device-resident line list (structure of arrays, ascending nu). */

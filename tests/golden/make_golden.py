@@ -50,7 +50,7 @@ def build_case(kind, p):
     return lines, grid, cond
 
 
-def main(which: str):
+def main(which: str, outdir: str = HERE):
     for name, (kind, p) in CASES.items():
         lines, grid, cond = build_case(kind, p)
         fr = grid.freq()
@@ -61,10 +61,10 @@ def main(which: str):
             for thr in (1, 4):
                 out[f"ref_cpu_t{thr}"] = oracle.ref_cpu(prof, fr, z, lines, cond, grid.dfreq,
                                                         nthreads=thr)
-            path = os.path.join(HERE, f"{name}.cpu.npz")
+            path = os.path.join(outdir, f"{name}.cpu.npz")
         else:
             out["ref_gpu"], _ = oracle.ref_gpu(prof, fr, z, lines, cond, grid.dfreq)
-            path = os.path.join(HERE, f"{name}.gpu.npz")
+            path = os.path.join(outdir, f"{name}.gpu.npz")
         np.savez_compressed(path, nu=lines.nu, energies=lines.energies, aif=lines.aif,
                             gns=lines.gns, gamma=lines.gamma, n=lines.n, grid=np.array(p["grid"]),
                             temperature=cond["temperature"], partition=cond["partition"],
@@ -74,4 +74,6 @@ def main(which: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "cpu")
+    out = sys.argv[2] if len(sys.argv) > 2 else HERE
+    os.makedirs(out, exist_ok=True)
+    main(sys.argv[1] if len(sys.argv) > 1 else "cpu", out)

@@ -78,5 +78,7 @@ def test_scratch_bytes_needed_scales_with_lines_and_conditions(built_libs):
     a = capi.lib().xs_scratch_bytes_needed(ctypes.byref(o), 1, 1_000_000)
     b = capi.lib().xs_scratch_bytes_needed(ctypes.byref(o), 4, 1_000_000)
     c = capi.lib().xs_scratch_bytes_needed(ctypes.byref(o), 1, 2_000_000)
-    assert 80_000_000 <= a <= 100_000_000  # 48 + 32 + 8 bytes per line
-    assert abs(b - 4 * a) < 4096 and abs(c - 2 * a) < 4096
+    # per line and condition: a 64-byte record and a window (8 bytes); per
+    # line: its nearest grid index (4 bytes)
+    assert abs(a - 76 * 1_000_000) < 4096
+    assert abs(b - (4 * 72 + 4) * 1_000_000) < 4096 and abs(c - 2 * a) < 4096

@@ -134,14 +134,40 @@ def test_mixed_precision_pressure_regimes(engine, cuda, p_bar):
 
 
 def test_multi_condition_batch_matches_single_runs(engine, cuda):
+    """A batch of conditions gives each condition's single-run result (the
+    multi-condition tiles sum in another fixed order: FP64 rounding only)."""
     lines, grid, cond = small_voigt_case(seed=41, n=1500)
     fr = grid.freq()
     conds = [dict(cond, temperature=t, partition=synth.partition_poly(t), gamma_scale=p, cut=25.0)
              for t in (300.0, 1200.0) for p in (0.01, 1.0, 5.0)]
     batch = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, conds=conds)
+    again = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, conds=conds)
+    assert np.array_equal(batch, again)  # deterministic
     for k, c in enumerate(conds):
         single = run_engine(engine, capi.VOIGT, lines, fr, c, grid.dfreq, cuda)
-        assert np.array_equal(batch[k], single)
+        assert_fp64_parity(batch[k], single, rel=1e-12)
+
+
+@pytest.mark.parametrize("C", [2, 4])
+def test_multi_condition_tiles_vs_oracle(engine, cuda, C):
+    """Forced multi-condition tiles: FP64 against the oracle per condition,
+    mixed against FP64, across Doppler- and pressure-dominated conditions."""
+    lines = synth.random_lines(2500, 1000.0, 1100.0, 2500.0, 1e-6, 1e2, seed=51, pressure_atm=1.0)
+    grid = synth.Grid(990.0, 1110.0, 1200)  # 0.1 cm-1, as in the sweep
+    base = dict(mean_mass=17.03, pressure=1.0, ref_temp=296.0)
+    conds = [dict(base, temperature=t, partition=synth.partition_poly(t), gamma_scale=p, cut=25.0)
+             for t in (300.0, 2100.0) for p in (1e-3, 10.0)]
+    fr = grid.freq()
+    f64 = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, C=C)
+    mix = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, C=C,
+                     precision=capi.MIXED)
+    for k, c in enumerate(conds):
+        scaled = synth.LineList(lines.nu, lines.energies, lines.aif, lines.gns,
+                                lines.gamma * c["gamma_scale"], lines.n)
+        ref = oracle.gpu_convention(oracle.VOIGT, fr, np.zeros_like(fr), scaled,
+                                    dict(c, pressure=1.0), grid.dfreq)
+        assert_fp64_parity(f64[k], ref)
+        assert_mixed_parity(mix[k], f64[k])
 
 
 def test_empty_and_outside_lines(engine, cuda):
