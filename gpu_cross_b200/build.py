@@ -3,6 +3,7 @@
   libxsec_b200.so   CUDA kernels for sm_100a + the C ABI (include/xsec_b200.h)
   libxsec_host.so   C++ host layer mirroring the reference's classes
                     (include/xsec/*.h) on top of the C ABI
+  xsec_cross        the reference's main program on that layer
 
 nvcc cross-compiles for sm_100a without a GPU.  Objects are rebuilt when a
 source or header is newer than the library.
@@ -22,6 +23,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIBDIR = os.path.join(PKG, "lib")
 LIB_CUDA = os.path.join(LIBDIR, "libxsec_b200.so")
 LIB_HOST = os.path.join(LIBDIR, "libxsec_host.so")
+CLI = os.path.join(LIBDIR, "xsec_cross")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 CXX = os.environ.get("CXX", "g++")
@@ -58,13 +60,18 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if force or _newer(LIB_CUDA, objs):
         _run([NVCC, *GENCODE, "-shared", "-o", LIB_CUDA, *objs, "-lcudart"], verbose)
 
-    host_srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
+    host_srcs = sorted(p for p in glob.glob(os.path.join(HOST, "*.cpp"))
+                       if os.path.basename(p) != "main.cpp")
     if host_srcs:
         host_headers = glob.glob(os.path.join(INCLUDE, "xsec", "*.h")) + headers
         if force or _newer(LIB_HOST, [*host_srcs, *host_headers, LIB_CUDA]):
-            _run([CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-I", INCLUDE, "-o", LIB_HOST,
-                  *host_srcs, "-L", LIBDIR, "-lxsec_b200", "-Wl,-rpath,$ORIGIN", "-pthread"],
-                 verbose)
+            _run([CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-I", INCLUDE, "-o",
+                  LIB_HOST, *host_srcs, "-L", LIBDIR, "-lxsec_b200", "-Wl,-rpath,$ORIGIN",
+                  "-ldl", "-pthread"], verbose)
+        main = os.path.join(HOST, "main.cpp")
+        if os.path.exists(main) and (force or _newer(CLI, [main, *host_headers, LIB_HOST])):
+            _run([CXX, "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, "-o", CLI, main, "-L", LIBDIR,
+                  "-lxsec_host", "-lxsec_b200", "-Wl,-rpath,$ORIGIN", "-pthread"], verbose)
     return LIB_CUDA
 
 

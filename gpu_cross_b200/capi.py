@@ -69,6 +69,7 @@ _SIGS = {
     "xs_last_error": (ctypes.c_char_p, []),
     "xs_version": (ctypes.c_char_p, []),
     "xs_device_available": (_I, []),
+    "xs_device_count": (_I, [ctypes.POINTER(ctypes.c_int)]),
     "xs_copy_intensity_info": (_I, [ctypes.POINTER(CrossSectionData)]),
     "xs_execute_two_step_kernal_voigt_block": (_I, [_VP] * 8 + [_I, _I, _I]),
     "xs_execute_two_step_kernal_doppler_block": (_I, [_VP] * 6 + [_I, _I, _I]),

@@ -153,6 +153,18 @@ int xs_device_available(void) {
     return 0;
 }
 
+int xs_device_count(int* count) {
+    if (!count) return fail(XS_ERR_INVALID, "xs_device_count: count is NULL");
+    *count = 0;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return XS_OK;
+    }
+    *count = n;
+    return XS_OK;
+}
+
 int xs_engine_create(int device, xs_engine** out) {
     if (!out) return fail(XS_ERR_INVALID, "xs_engine_create: out is NULL");
     *out = nullptr;

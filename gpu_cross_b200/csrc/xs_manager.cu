@@ -152,7 +152,9 @@ int xs_manager_initialize_vectors(xs_manager* m, int Npoints) {
     XM_CU(cudaMalloc(&m->d_intens, sizeof(double) * size_t(Npoints)));
     XM_CU(cudaMemset(m->d_intens, 0, sizeof(double) * size_t(Npoints)));
     m->npoints = Npoints;
-    const size_t raw = (m->profile == XS_VOIGT) ? 44 : 36;  // bytes per line (GPUManager.cpp:55-58)
+    // bytes per line: nu, E, A, gns (+ gamma, n for Voigt), GPUManager.cpp:55-58
+    // and OpenMPManager.cpp:32-35
+    const size_t raw = (m->profile == XS_VOIGT) ? 44 : 28;
     if (m->kind == 1) {
         // OpenMPManager::InitializeVectors (OpenMPManager.cpp:9, 19-35): half
         // of total_memory, minus the grids, divided by the bytes per line.

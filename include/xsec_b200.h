@@ -134,6 +134,11 @@ const char* xs_last_error(void);
 const char* xs_version(void);
 /* 1 if a usable sm_100 device is present (no context is created otherwise). */
 int xs_device_available(void);
+/* Number of visible CUDA devices (0 when there is no driver or device).  The
+ * reference's MultiGpuManager (MultiGPUManager.cpp:5-16) makes one manager per
+ * device; xs_manager_create reports XS_ERR_NODEVICE for a device that is not
+ * sm_100. */
+int xs_device_count(int* count);
 
 /* ---- 1. launcher level: drop-in for cross_kernal.cuh -------------------- */
 /* copy_intensity_info (cross_kernal.cuh:18): per-device constants used by the

@@ -1,0 +1,76 @@
+"""End to end on the B200: xsec_cross (the reference's main program on the
+C++ host layer) reads each synthetic case's .inp, ExoMol/HITRAN files and
+.bz2 streams, chunks the lines, computes on the GPU and prints the
+spectrum.  The default backend (HybridManager, the reference's CPU
+arithmetic) must print what the reference's own main program printed
+(tests/golden/e2e_*.spec.xz); the GPU-convention backends must match the
+oracle's restatement of the reference GPU kernels; mixed precision must meet
+its accuracy bounds."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import e2e_cases
+import oracle
+from helpers import MIXED_INTEGRATED, MIXED_REL, PEAK_FLOOR
+from test_host_layer import PRINT_REL, case_lines, cli, load_golden
+
+pytestmark = pytest.mark.gpu
+
+CASES = sorted(e2e_cases.CASES)
+
+
+def run_cli(workdir, *args):
+    p = cli(["--input", "case.inp", *args], workdir)
+    assert p.returncode == 0, p.stderr[-2000:]
+    fr, iv = e2e_cases.parse_spectrum(p.stdout)
+    return fr, iv, p.stderr
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_cli_prints_the_reference_programs_spectrum(cuda, tmp_path, name):
+    lines, cond, grid, prof, thr = case_lines(name, tmp_path)
+    _, want = load_golden(name)
+    fr, got, log = run_cli(tmp_path)
+    assert len(got) == grid.npoints
+    np.testing.assert_allclose(fr, grid.freq(), rtol=0, atol=5e-7)
+    peak = np.abs(want).max()
+    err = np.abs(got - want)
+    assert np.all(err <= PRINT_REL * np.abs(want) + 1e-12 * peak), float((err / peak).max())
+    if name == "exomol_voigt":
+        # MAX-POINTS 3000 over a 20000-point grid: several chunks
+        assert "in 1 chunks" not in log
+
+
+@pytest.mark.parametrize("backend", ["gpu", "multigpu"])
+@pytest.mark.parametrize("name", CASES)
+def test_cli_gpu_convention_backends(cuda, tmp_path, name, backend):
+    lines, cond, grid, prof, _ = case_lines(name, tmp_path)
+    want = oracle.gpu_convention(prof, grid.freq(), np.zeros(grid.npoints), lines, cond, grid.dfreq)
+    _, got, _ = run_cli(tmp_path, "--backend", backend)
+    peak = np.abs(want).max()
+    err = np.abs(got - want)
+    # one rounding of the printed value on top of the engine's <= 1e-10
+    assert np.all(err <= (PRINT_REL + 1e-10) * np.abs(want) + 1e-12 * peak), \
+        float((err / peak).max())
+
+
+@pytest.mark.parametrize("name", ["exomol_voigt", "hitran_voigt"])
+def test_cli_mixed_precision(cuda, tmp_path, name):
+    case_lines(name, tmp_path)
+    _, want = load_golden(name)
+    _, got, _ = run_cli(tmp_path, "--precision", "mixed")
+    peak = np.abs(want).max()
+    big = np.abs(want) > PEAK_FLOOR * peak
+    rel = np.abs(got[big] - want[big]) / np.abs(want[big])
+    assert rel.max() <= MIXED_REL
+    assert abs(got.sum() - want.sum()) / want.sum() <= MIXED_INTEGRATED
+    assert np.abs(got[~big] - want[~big]).max(initial=0.0) <= MIXED_REL * peak
+
+
+def test_cli_openmp_backend_equals_hybrid(cuda, tmp_path):
+    case_lines("hitran_voigt", tmp_path)
+    _, a, _ = run_cli(tmp_path)
+    _, b, _ = run_cli(tmp_path, "--backend", "openmp")
+    np.testing.assert_array_equal(a, b)
