@@ -497,6 +497,26 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     return XS_OK;
 }
 
+int engine_reserve(xs_engine* e, size_t bytes) {
+    if (!e) return fail(XS_ERR_INVALID, "engine_reserve: NULL engine");
+    std::lock_guard<std::mutex> lk(e->mu);
+    if (bytes <= e->scratch_cap) return XS_OK;
+    DeviceGuard dg(e->device);
+    XS_CU(cudaStreamSynchronize(e->stream));
+    cudaFree(e->scratch);
+    e->scratch = nullptr;
+    e->scratch_cap = 0;
+    cudaError_t err = cudaMalloc(&e->scratch, bytes);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(err, "cudaMalloc(scratch)");
+    }
+    e->scratch_cap = bytes;
+    return XS_OK;
+}
+
+int engine_device(const xs_engine* e) { return e ? e->device : -1; }
+
 }  // namespace xs
 
 struct xs_graph {

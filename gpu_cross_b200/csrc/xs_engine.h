@@ -26,6 +26,12 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
                    const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride,
                    const ExecOverride* ov);
 
+// Grows the engine's scratch to at least `bytes` (synchronises the engine's
+// stream when it has to reallocate).
+int engine_reserve(xs_engine* e, size_t bytes);
+// The engine's device and stream.
+int engine_device(const xs_engine* e);
+
 int set_error(int code, const char* msg);
 CondDev make_cond(const xs_options& o, const xs_condition& c);
 long cpu_covered_lines(long n, int threads);

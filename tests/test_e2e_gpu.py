@@ -8,6 +8,8 @@ oracle's restatement of the reference GPU kernels; mixed precision must meet
 its accuracy bounds."""
 from __future__ import annotations
 
+import re
+
 import numpy as np
 import pytest
 
@@ -43,12 +45,31 @@ def test_cli_prints_the_reference_programs_spectrum(cuda, tmp_path, name):
         assert "in 1 chunks" not in log
 
 
+def chunks_of(log):
+    """(lines, ib, ie) of every chunk the profile evaluated, from its log."""
+    out = []
+    for m in re.finditer(r"chunk \d+: (\d+) lines, points \[(-?\d+), (-?\d+)\)", log):
+        out.append(tuple(int(v) for v in m.groups()))
+    return out
+
+
 @pytest.mark.parametrize("backend", ["gpu", "multigpu"])
 @pytest.mark.parametrize("name", CASES)
 def test_cli_gpu_convention_backends(cuda, tmp_path, name, backend):
+    """GpuManager arithmetic through the profile's chunks: each chunk covers
+    the grid points [ib, ie) (BaseProfile.cpp:55-60), so a window point that
+    rounds outside its chunk is not evaluated -- as in the reference."""
     lines, cond, grid, prof, _ = case_lines(name, tmp_path)
-    want = oracle.gpu_convention(prof, grid.freq(), np.zeros(grid.npoints), lines, cond, grid.dfreq)
-    _, got, _ = run_cli(tmp_path, "--backend", backend)
+    _, got, log = run_cli(tmp_path, "--backend", backend)
+    want = np.zeros(grid.npoints)
+    k = 0
+    chunks = chunks_of(log)
+    assert chunks and sum(c[0] for c in chunks) == len(lines)
+    for n, ib, ie in chunks:
+        if ie > ib:
+            want = oracle.gpu_convention(prof, grid.freq(), want, lines.slice(k, k + n), cond,
+                                         grid.dfreq, points=ie - ib, start_idx=ib)
+        k += n
     peak = np.abs(want).max()
     err = np.abs(got - want)
     # one rounding of the printed value on top of the engine's <= 1e-10
