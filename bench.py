@@ -37,8 +37,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-FLOPS_PER_PAIR = 14  # algorithmic FLOPs of one Voigt region-I pair
-METRIC = "Voigt line-evals/s (mixed-precision batched 40-(T,P) sweep)"
+# algorithmic FLOPs of one Voigt region-I pair: offset, x^2, the real
+# rational's numerator and denominator, the scale and the accumulate, with the
+# per-line terms hoisted (the reciprocal runs on the XU pipe, not counted)
+FLOPS_PER_PAIR = 14
+METRIC = "Voigt line-evals/s & p99 request latency: mixed-precision batched vs plain FP64"
 
 
 def log(*a):
@@ -394,6 +397,15 @@ def run_ours(args, rank, world, dist):
     eng.close()
     if eng2 is not None:
         eng2.close()
+    del d, out, out_f64, out_host
+    torch.cuda.empty_cache()
+
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        try:
+            serving = run_serving(args, dev.index)
+        except Exception as exc:
+            serving = {"error": f"{type(exc).__name__}: {exc}"}
 
     if rank != 0:
         return None
@@ -439,10 +451,95 @@ def run_ours(args, rank, world, dist):
         "reference_gpu_kernel": ref_gpu,
         "e2e": {"value": e2e_value, "unit": "line-evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "serving": serving,
         "gpu_launches": 3 * args.steps,
         "clocks": clk,
         "when": datetime.datetime.now(datetime.timezone.utc).isoformat(),
     }
+
+
+def run_serving(args, dev_index: int):
+    """The request server under a seeded Poisson stream (three resident
+    molecules of 1e6, 1e7 and 1e8 lines), once with every request in mixed
+    precision and once in plain FP64.  Latency is the server's own: submit to
+    result in pinned host memory."""
+    import queue
+
+    from gpu_cross_b200 import capi, synth
+
+    t0 = time.perf_counter()
+    mols = synth.serving_molecules(args.serve_scale)
+    trace = synth.serving_trace(rate=args.serve_rate, duration_s=args.serve_seconds)
+    log(f"[serve] {len(mols)} molecules ({sum(len(l) for l, _ in mols):.3e} lines) and "
+        f"{len(trace)} requests generated in {time.perf_counter() - t0:.1f} s")
+    srv = capi.Server(dev_index)
+    try:
+        mids = [srv.add_molecule(l, m) for l, m in mols]
+        del mols
+
+        def submit(r, prec):
+            return srv.submit(mids[r["molecule"]], capi.VOIGT if r["voigt"] else capi.DOPPLER, prec,
+                              r["temperature"], r["partition"], r["pressure"], r["f0"], r["df"],
+                              r["npoints"], cut=r["cut"])
+
+        def stream(prec):
+            q: queue.Queue = queue.Queue()
+            infos = []
+            done_at = []
+
+            def waiter():
+                while True:
+                    item = q.get()
+                    if item is None:
+                        return
+                    rid, n = item
+                    _, info = srv.wait(rid, n)
+                    infos.append(info)
+                    done_at.append(time.perf_counter())
+
+            th = threading.Thread(target=waiter)
+            th.start()
+            late = []
+            start = time.perf_counter()
+            for r in trace:
+                dt = r["t"] - (time.perf_counter() - start)
+                if dt > 0:
+                    time.sleep(dt)
+                late.append(time.perf_counter() - start - r["t"])
+                q.put((submit(r, prec), r["npoints"]))
+            q.put(None)
+            th.join()
+            span = max(done_at) - start
+            lat = np.array([i["latency_ms"] for i in infos])
+            evals = float(sum(i["line_evals"] for i in infos))
+            vo = np.array([r["voigt"] for r in trace])
+            return {
+                "requests": len(infos), "seconds": span,
+                "requests_per_s": len(infos) / span,
+                "line_evals_per_s": evals / span,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "max_ms": float(lat.max()), "mean_ms": float(lat.mean()),
+                "p99_ms_voigt": float(np.percentile(lat[vo], 99)) if vo.any() else None,
+                "p99_ms_doppler": float(np.percentile(lat[~vo], 99)) if (~vo).any() else None,
+                "queue_p99_ms": float(np.percentile([i["queue_ms"] for i in infos], 99)),
+                "submit_late_p99_ms": float(np.percentile(late, 99) * 1e3),
+                "chunks": int(sum(i["chunks"] for i in infos)),
+            }
+
+        # warm-up: the first requests of the trace, one at a time
+        for r in trace[:16]:
+            srv.wait(submit(r, capi.MIXED), r["npoints"])
+            srv.wait(submit(r, capi.FP64), r["npoints"])
+        res = {"mixed": stream(capi.MIXED), "fp64": stream(capi.FP64)}
+    finally:
+        srv.close()
+    res["config"] = (f"{len(trace)} requests, Poisson {args.serve_rate:g}/s over "
+                     f"{args.serve_seconds:g} s (seed 1005); molecules "
+                     f"{'/'.join(f'{n * args.serve_scale:.0e}' for n, _ in synth.SERVE_MOLECULES)} "
+                     "lines (M 18.02/30.01/16.04), T U(200,3000) K, P logU(1e-5,100) bar, "
+                     "Doppler/Voigt 1:1, span U(100,5000) cm-1, df logU(0.01,1) cm-1, cut 25")
+    res["line_evals"] = "window-overlap count (line, point) pairs inside +/-25 cm-1"
+    return res
 
 
 def run_reference(args, rank, world):
@@ -506,6 +603,11 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--conds", type=int, default=40, help="subset of the 40 conditions (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-serve", action="store_true", help="skip the request-server stream")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-scale", type=float, default=1.0,
+                    help="scale of the served molecules' line counts (1 = 1e6/1e7/1e8)")
     args = ap.parse_args()
     if not args.points:
         args.points = 750_000 if args.workload == "single" else 75_000

@@ -59,6 +59,25 @@ class GridC(ctypes.Structure):
                 ("start_idx", ctypes.c_int), ("points", ctypes.c_int)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device_budget", ctypes.c_size_t), ("host_budget", ctypes.c_size_t),
+                ("lanes", ctypes.c_int), ("depth", ctypes.c_int), ("chunk_pairs", ctypes.c_double),
+                ("chunk_lines", ctypes.c_size_t)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("molecule", ctypes.c_int), ("profile", ctypes.c_int), ("precision", ctypes.c_int),
+                ("temperature", ctypes.c_double), ("partition", ctypes.c_double),
+                ("pressure", ctypes.c_double), ("cut", ctypes.c_double), ("f0", ctypes.c_double),
+                ("df", ctypes.c_double), ("npoints", ctypes.c_int)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("latency_ms", ctypes.c_double),
+                ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("chunks", ctypes.c_int),
+                ("line_evals", ctypes.c_double), ("lines", ctypes.c_size_t)]
+
+
 _VP = ctypes.c_void_p
 _I = ctypes.c_int
 _D = ctypes.c_double
@@ -104,6 +123,14 @@ _SIGS = {
     "xs_manager_cleanup": (_I, [_VP]),
     "xs_manager_ready_for_work": (_I, [_VP, ctypes.POINTER(_I)]),
     "xs_manager_get_ntrans": (_I, [_VP, ctypes.POINTER(_SZ)]),
+    "xs_server_create": (_I, [_I, ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
+    "xs_server_destroy": (_I, [_VP]),
+    "xs_server_add_molecule": (_I, [_VP] + [_VP] * 6 + [_SZ, _D, _D, ctypes.POINTER(_I)]),
+    "xs_server_submit": (_I, [_VP, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_ulonglong)]),
+    "xs_server_wait": (_I, [_VP, ctypes.c_ulonglong, _VP, _I, ctypes.POINTER(RequestInfo), _I]),
+    "xs_server_pending": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "xs_plan_chunks": (_I, [_VP, _SZ, _D, _D, _I, _D, _D, _SZ, _I, _VP, _VP, _VP, _VP, _VP,
+                            ctypes.POINTER(_I)]),
 }
 
 _lib: ctypes.CDLL | None = None
@@ -321,3 +348,83 @@ class Manager:
         v = ctypes.c_size_t()
         check(lib().xs_manager_get_ntrans(self.h, ctypes.byref(v)))
         return int(v.value)
+
+
+# ---------------------------------------------------------------------------
+def plan_chunks(nu, f0: float, df: float, npoints: int, cut: float, max_pairs: float,
+                max_lines: int = 0):
+    """The server's chunk planner on a host nu array (no device needed).
+    Returns a dict of numpy arrays: start, points, l0, l1, pairs."""
+    import numpy as np
+
+    nu = np.ascontiguousarray(nu, dtype=np.float64)
+    cap = npoints // 256 + 2
+    out = dict(start=np.zeros(cap, np.int32), points=np.zeros(cap, np.int32),
+               l0=np.zeros(cap, np.uint64), l1=np.zeros(cap, np.uint64), pairs=np.zeros(cap))
+    n = ctypes.c_int()
+    check(lib().xs_plan_chunks(nu.ctypes.data if nu.size else None, nu.size, f0, df, npoints, cut,
+                               max_pairs, max_lines, cap, out["start"].ctypes.data,
+                               out["points"].ctypes.data, out["l0"].ctypes.data,
+                               out["l1"].ctypes.data, out["pairs"].ctypes.data, ctypes.byref(n)))
+    return {k: v[:n.value] for k, v in out.items()}
+
+
+class Server:
+    """A request server (xs_server_*): resident molecules, submit/wait."""
+
+    def __init__(self, device: int = 0, device_budget: int = 0, host_budget: int = 0,
+                 lanes: int = 0, depth: int = 0, chunk_pairs: float = 0.0, chunk_lines: int = 0):
+        cfg = ServerConfig(device_budget, host_budget, lanes, depth, chunk_pairs, chunk_lines)
+        h = ctypes.c_void_p()
+        check(lib().xs_server_create(device, ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().xs_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_molecule(self, lines, mean_mass: float, ref_temp: float = 296.0) -> int:
+        """lines: a synth.LineList (host numpy arrays, nu ascending, gamma per atm)."""
+        import numpy as np
+
+        arrs = [np.ascontiguousarray(lines.nu, np.float64),
+                np.ascontiguousarray(lines.energies, np.float64),
+                np.ascontiguousarray(lines.aif, np.float64),
+                np.ascontiguousarray(lines.gns, np.int32),
+                np.ascontiguousarray(lines.gamma, np.float64),
+                np.ascontiguousarray(lines.n, np.float64)]
+        mid = ctypes.c_int()
+        check(lib().xs_server_add_molecule(self.h, *[a.ctypes.data for a in arrs], arrs[0].size,
+                                           mean_mass, ref_temp, ctypes.byref(mid)))
+        return mid.value
+
+    def submit(self, molecule: int, profile: int, precision: int, temperature: float,
+               partition: float, pressure: float, f0: float, df: float, npoints: int,
+               cut: float = -1.0) -> int:
+        r = Request(molecule, profile, precision, temperature, partition, pressure, cut, f0, df,
+                    npoints)
+        rid = ctypes.c_ulonglong()
+        check(lib().xs_server_submit(self.h, ctypes.byref(r), ctypes.byref(rid)))
+        return rid.value
+
+    def wait(self, rid: int, npoints: int, timeout_ms: int = -1):
+        """(result as numpy float64[npoints], info dict)."""
+        import numpy as np
+
+        out = np.empty(npoints, np.float64)
+        info = RequestInfo()
+        check(lib().xs_server_wait(self.h, rid, out.ctypes.data, npoints, ctypes.byref(info),
+                                   timeout_ms))
+        return out, {k: getattr(info, k) for k, _ in RequestInfo._fields_}
+
+    def pending(self):
+        q, a = ctypes.c_int(), ctypes.c_int()
+        check(lib().xs_server_pending(self.h, ctypes.byref(q), ctypes.byref(a)))
+        return q.value, a.value

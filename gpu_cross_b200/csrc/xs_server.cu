@@ -1,0 +1,845 @@
+// Request server: continuous batching of cross-section requests over line
+// lists kept resident in HBM.  No counterpart in the reference (which runs
+// one .inp job per process); it serves the same arithmetic per request.
+//
+// A request names a resident molecule, T, Q(T), P, a profile and a uniform
+// grid.  Its grid is planned into chunks of whole 256-point tiles, each with
+// the slice of lines that can reach it and bounded work, so that no chunk
+// holds the GPU for long.  A scheduler thread
+//   * admits queued requests (FIFO) while their device and pinned-host
+//     memory fit the budgets, giving each a lane (stream + engine) and
+//     filling its grid and zeroing its output on that stream;
+//   * issues chunks to every lane that has room, the request with the least
+//     remaining work first, so small requests that arrive while a large one
+//     runs are interleaved between its chunks and finish early;
+//   * after a request's last chunk, copies its result to pinned host memory
+//     and, when that copy's event completes, releases its memory and wakes
+//     the waiter.
+// Work from different lanes overlaps on the device.  A request's chunks
+// depend only on the request itself, so its result is bit-identical whether
+// it runs alone or in a mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "xs_engine.h"
+#include "xsec_b200.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+int sfail(int code, const std::string& msg) { return xs::set_error(code, msg.c_str()); }
+
+// f[i] = f0 + i*df with one rounding per operation (no fused multiply-add),
+// the grid BaseProfile builds (BaseProfile.cpp:17-21).
+__global__ void k_fill_grid(double* f, double f0, double df, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) f[i] = __dadd_rn(f0, __dmul_rn(double(i), df));
+}
+
+constexpr int kTile = 256;  // chunk granularity: a multiple of every tile width
+// Molecules per server.  The scheduler reads the molecule table without the
+// lock; reserving it up front keeps its elements in place while
+// xs_server_add_molecule appends.
+constexpr size_t kMaxMolecules = 64;
+
+// ---------------------------------------------------------------------------
+// Chunk planning (host only).
+//
+// Line-evals of a 256-point tile [a, b] (a = f_s - df/2, b = f_e-1 + df/2)
+// are estimated as the summed overlap of the windows [nu - cut, nu + cut]
+// with [a, b], divided by df.  On each interval between the four breakpoints
+// a -/+ cut, b -/+ cut the overlap is linear in nu, so prefix sums of nu
+// give the sum from four lower-bound positions; the sum is additive over
+// tiles.  The breakpoints only move up from tile to tile, so each position
+// is found by a galloping search from the previous tile's.
+struct LineIndex {
+    const double* nu = nullptr;   // ascending
+    const double* cum = nullptr;  // cum[k] = sum of nu[0..k)
+    size_t n = 0;
+
+    size_t lower(double v) const { return size_t(std::lower_bound(nu, nu + n, v) - nu); }
+    size_t upper(double v) const { return size_t(std::upper_bound(nu, nu + n, v) - nu); }
+};
+
+// First index with nu[i] >= v (strict = false) or nu[i] > v (strict = true),
+// for nondecreasing v.
+struct Cursor {
+    size_t pos = 0;
+    size_t seek(const LineIndex& L, double v, bool strict) {
+        auto before = [&](size_t i) { return strict ? !(L.nu[i] > v) : L.nu[i] < v; };
+        if (pos >= L.n || !before(pos)) return pos;
+        size_t lo = pos, step = 1, hi;
+        for (;;) {  // before(lo) holds
+            hi = lo + step;
+            if (hi >= L.n) {
+                hi = L.n;
+                break;
+            }
+            if (!before(hi)) break;
+            lo = hi;
+            step *= 2;
+        }
+        const double* first = L.nu + lo + 1;
+        const double* last = L.nu + hi;
+        pos = size_t((strict ? std::upper_bound(first, last, v) : std::lower_bound(first, last, v)) - L.nu);
+        return pos;
+    }
+};
+
+double overlap_sum(const LineIndex& L, const size_t idx[4], const double p[4], double a, double b,
+                   double cut) {
+    double sum = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        if (!(p[k + 1] > p[k])) continue;
+        const size_t i0 = idx[k], i1 = idx[k + 1];
+        if (i1 <= i0) continue;
+        const double mid = 0.5 * (p[k] + p[k + 1]);
+        const bool min_nu = mid + cut < b;  // min(nu + cut, b) is nu + cut
+        const bool max_nu = mid - cut > a;  // max(nu - cut, a) is nu - cut
+        const double slope = (min_nu ? 1.0 : 0.0) - (max_nu ? 1.0 : 0.0);
+        const double icpt = (min_nu ? cut : b) - (max_nu ? -cut : a);
+        const double v = slope * (L.cum[i1] - L.cum[i0]) + icpt * double(i1 - i0);
+        if (v > 0.0) sum += v;
+    }
+    return sum;
+}
+
+struct ChunkPlan {
+    int start, points;
+    size_t l0, l1;  // line slice
+    double pairs;   // estimated line-evals
+};
+
+// Greedy over tiles: a chunk takes tiles while its estimated line-evals stay
+// within max_pairs and its line slice within max_lines (at least one tile).
+void plan_chunks(const LineIndex& L, double f0, double df, int npoints, double cut,
+                 double max_pairs, size_t max_lines, std::vector<ChunkPlan>& out) {
+    out.clear();
+    const double margin = 2.0 * df;
+    auto freq = [&](long i) { return f0 + double(i) * df; };
+    Cursor bp[4], c_lo, c_hi;
+    const int ntiles = (npoints + kTile - 1) / kTile;
+    ChunkPlan cur{0, 0, 0, 0, 0.0};
+    for (int t = 0; t < ntiles; ++t) {
+        const int s = t * kTile, e = std::min(npoints, s + kTile);
+        const double a = freq(s) - 0.5 * df, b = freq(e - 1) + 0.5 * df;
+        // breakpoints in ascending order; a + cut and b - cut swap when the
+        // tile is wider than the window
+        double p[4] = {a - cut, std::min(a + cut, b - cut), std::max(a + cut, b - cut), b + cut};
+        size_t idx[4];
+        for (int k = 0; k < 4; ++k) idx[k] = bp[k].seek(L, p[k], false);
+        const double tp = overlap_sum(L, idx, p, a, b, cut) / df;
+        const size_t l1 = c_hi.seek(L, freq(e - 1) + cut + margin, true);
+        if (cur.points > 0 && (cur.pairs + tp > max_pairs || l1 - cur.l0 > max_lines)) {
+            out.push_back(cur);
+            cur = ChunkPlan{s, 0, 0, 0, 0.0};
+        }
+        if (cur.points == 0) {
+            cur.start = s;
+            cur.l0 = c_lo.seek(L, freq(s) - cut - margin, false);
+        }
+        cur.points = e - cur.start;
+        cur.l1 = l1;
+        cur.pairs += tp;
+    }
+    out.push_back(cur);
+}
+
+// ---------------------------------------------------------------------------
+// First-fit allocator over one pinned host arena.
+class Arena {
+public:
+    bool init(size_t bytes) {
+        if (cudaHostAlloc(&base_, bytes, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            base_ = nullptr;
+            return false;
+        }
+        size_ = bytes;
+        free_[0] = bytes;
+        return true;
+    }
+    void release() {
+        if (base_) cudaFreeHost(base_);
+        base_ = nullptr;
+        free_.clear();
+    }
+    // Returns the offset, or SIZE_MAX when nothing fits.
+    size_t alloc(size_t bytes) {
+        bytes = (bytes + 255) & ~size_t(255);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= bytes) {
+                const size_t off = it->first, left = it->second - bytes;
+                free_.erase(it);
+                if (left) free_[off + bytes] = left;
+                used_ += bytes;
+                return off;
+            }
+        }
+        return SIZE_MAX;
+    }
+    void free(size_t off, size_t bytes) {
+        bytes = (bytes + 255) & ~size_t(255);
+        used_ -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    double* at(size_t off) { return reinterpret_cast<double*>(static_cast<char*>(base_) + off); }
+    size_t size() const { return size_; }
+
+private:
+    void* base_ = nullptr;
+    size_t size_ = 0, used_ = 0;
+    std::map<size_t, size_t> free_;
+};
+
+struct Molecule {
+    double *nu = nullptr, *e = nullptr, *a = nullptr, *g = nullptr, *nx = nullptr;
+    int* gns = nullptr;
+    size_t n = 0;
+    double mass = 0.0, ref_temp = 296.0;
+    std::vector<double> h_nu, h_cum;
+    size_t bytes = 0;
+    LineIndex index() const {
+        LineIndex L;
+        L.nu = h_nu.data();
+        L.cum = h_cum.data();
+        L.n = n;
+        return L;
+    }
+};
+
+struct Request {
+    unsigned long long id = 0;
+    xs_request q{};
+    xs_options opt{};
+    xs_condition cond{};
+    std::vector<ChunkPlan> chunks;
+    size_t next = 0;
+    int lane = -1;
+    double remaining = 0.0, pairs = 0.0;
+    size_t lines = 0;
+    double* d_freq = nullptr;
+    double* d_out = nullptr;
+    size_t dev_bytes = 0, host_off = SIZE_MAX, host_bytes = 0;
+    Clock::time_point t_submit, t_admit, t_done;
+    int status = XS_OK;
+    std::string error;
+    bool done = false;
+};
+
+struct Flight {
+    Request* r;
+    cudaEvent_t ev;
+    bool last;
+};
+
+struct Lane {
+    xs_engine* eng = nullptr;
+    cudaStream_t st = nullptr;
+    std::deque<Flight> flight;
+    double load = 0.0;  // remaining line-evals of the requests assigned here
+};
+
+}  // namespace
+
+struct xs_server {
+    int device = 0;
+    xs_server_config cfg{};
+    size_t resident = 0;        // molecules + lane scratch
+    size_t dev_requests = 0;    // grids + outputs of admitted requests
+    std::vector<Molecule> mols;
+    std::vector<Lane> lanes;
+    Arena arena;
+    std::vector<cudaEvent_t> ev_pool;
+
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> incoming;             // submitted, not yet seen by the scheduler
+    std::map<unsigned long long, Request*> all; // not yet collected by xs_server_wait
+    unsigned long long next_id = 1;
+    std::string fatal;
+
+    std::deque<Request*> queue;   // scheduler-owned: waiting for admission
+    std::vector<Request*> active; // scheduler-owned: admitted, not finished
+    std::thread worker;
+    std::atomic<bool> stop{false};
+    std::atomic<int> n_queued{0}, n_active{0};
+};
+
+namespace {
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DevGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+size_t request_device_bytes(const xs_request& q) {
+    const size_t b = sizeof(double) * size_t(q.npoints);
+    return 2 * ((b + 511) & ~size_t(511));
+}
+
+cudaEvent_t take_event(xs_server* s) {
+    if (!s->ev_pool.empty()) {
+        cudaEvent_t e = s->ev_pool.back();
+        s->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+
+void finish(xs_server* s, Request* r) {
+    Lane& ln = s->lanes[size_t(r->lane)];
+    if (r->d_freq) cudaFreeAsync(r->d_freq, ln.st);
+    if (r->d_out) cudaFreeAsync(r->d_out, ln.st);
+    r->d_freq = r->d_out = nullptr;
+    s->dev_requests -= r->dev_bytes;
+    ln.load -= r->remaining;
+    r->remaining = 0.0;
+    s->active.erase(std::find(s->active.begin(), s->active.end(), r));
+    s->n_active = int(s->active.size());
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->t_done = Clock::now();
+    r->done = true;
+    s->cv_done.notify_all();
+}
+
+// Marks every unfinished request failed (a CUDA error left the context
+// unusable) and stops the scheduler.
+void fail_all(xs_server* s, const std::string& why) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->fatal = why;
+    auto fail_one = [&](Request* r) {
+        r->status = XS_ERR_CUDA;
+        r->error = why;
+        r->t_done = Clock::now();
+        r->done = true;
+    };
+    for (Request* r : s->queue) fail_one(r);
+    for (Request* r : s->active) fail_one(r);
+    for (Request* r : s->incoming) fail_one(r);
+    s->queue.clear();
+    s->active.clear();
+    s->incoming.clear();
+    s->n_active = 0;
+    s->n_queued = 0;
+    s->cv_done.notify_all();
+}
+
+void fail_request(xs_server* s, Request* r, int code, const std::string& why) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->status = code;
+    r->error = why;
+    r->t_done = Clock::now();
+    r->done = true;
+    s->cv_done.notify_all();
+}
+
+enum class Admit { kAdmitted, kNoRoom, kFailed };
+
+Admit admit(xs_server* s, Request* r) {
+    const size_t host = sizeof(double) * size_t(r->q.npoints);
+    if (s->resident + s->dev_requests + r->dev_bytes > s->cfg.device_budget) return Admit::kNoRoom;
+    size_t off;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);  // the arena is shared with xs_server_wait
+        off = s->arena.alloc(host);
+    }
+    if (off == SIZE_MAX) return Admit::kNoRoom;
+    // the lane with the least outstanding work
+    size_t li = 0;
+    for (size_t k = 1; k < s->lanes.size(); ++k)
+        if (s->lanes[k].load < s->lanes[li].load) li = k;
+    Lane& ln = s->lanes[li];
+    r->lane = int(li);
+    r->host_off = off;
+    r->host_bytes = host;
+    const size_t half = r->dev_bytes / 2;
+    cudaError_t err = cudaMallocAsync(reinterpret_cast<void**>(&r->d_freq), half, ln.st);
+    if (err == cudaSuccess) err = cudaMallocAsync(reinterpret_cast<void**>(&r->d_out), half, ln.st);
+    if (err == cudaSuccess) {
+        const int n = r->q.npoints;
+        k_fill_grid<<<(n + 255) / 256, 256, 0, ln.st>>>(r->d_freq, r->q.f0, r->q.df, n);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemsetAsync(r->d_out, 0, sizeof(double) * size_t(r->q.npoints), ln.st);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        if (r->d_freq) cudaFreeAsync(r->d_freq, ln.st);
+        if (r->d_out) cudaFreeAsync(r->d_out, ln.st);
+        r->d_freq = r->d_out = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->arena.free(off, host);
+        }
+        r->host_off = SIZE_MAX;
+        fail_request(s, r, err == cudaErrorMemoryAllocation ? XS_ERR_NOMEM : XS_ERR_CUDA,
+                     std::string("admission: ") + cudaGetErrorString(err));
+        return Admit::kFailed;
+    }
+    s->dev_requests += r->dev_bytes;
+    ln.load += r->remaining;
+    r->t_admit = Clock::now();
+    s->active.push_back(r);
+    s->n_active = int(s->active.size());
+    return Admit::kAdmitted;
+}
+
+// Enqueues the next chunk of r on its lane.  Returns false on a CUDA error
+// that leaves the server unusable.
+bool issue(xs_server* s, Request* r) {
+    Lane& ln = s->lanes[size_t(r->lane)];
+    const Molecule& m = s->mols[size_t(r->q.molecule)];
+    const ChunkPlan& c = r->chunks[r->next++];
+    if (r->status == XS_OK) {
+        xs_lines L;
+        L.nu = m.nu + c.l0;
+        L.energies = m.e + c.l0;
+        L.aif = m.a + c.l0;
+        L.gns = m.gns + c.l0;
+        L.gamma = m.g + c.l0;
+        L.n = m.nx + c.l0;
+        L.count = c.l1 - c.l0;
+        xs_grid G{r->d_freq, r->q.npoints, c.start, c.points};
+        xs::ExecOverride ov;
+        ov.no_timing = true;
+        const int rc = xs::engine_execute(ln.eng, &r->opt, &r->cond, 1, &L, &G, r->d_out, 0, &ov);
+        if (rc != XS_OK) {
+            r->status = rc;
+            r->error = xs_last_error();
+            if (rc == XS_ERR_CUDA) return false;
+            r->next = r->chunks.size();  // nothing more to run
+        }
+    }
+    r->remaining -= c.pairs;
+    ln.load -= c.pairs;
+    const bool last = r->next >= r->chunks.size();
+    if (last && r->status == XS_OK) {
+        if (cudaMemcpyAsync(s->arena.at(r->host_off), r->d_out, sizeof(double) * size_t(r->q.npoints),
+                            cudaMemcpyDeviceToHost, ln.st) != cudaSuccess)
+            return false;
+    }
+    cudaEvent_t ev = take_event(s);
+    if (!ev || cudaEventRecord(ev, ln.st) != cudaSuccess) return false;
+    ln.flight.push_back({r, ev, last});
+    return true;
+}
+
+void scheduler(xs_server* s) {
+    DevGuard dg(s->device);
+    const int depth = s->cfg.depth;
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            bool busy = !s->active.empty() || !s->queue.empty();
+            if (!busy && s->incoming.empty() && !s->stop)
+                s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            while (!s->incoming.empty()) {
+                s->queue.push_back(s->incoming.front());
+                s->incoming.pop_front();
+            }
+            if (s->stop) {
+                // shutting down: requests not admitted yet are refused (their
+                // memory may be held by results nobody will collect)
+                for (Request* r : s->queue) {
+                    r->status = XS_ERR_STATE;
+                    r->error = "server destroyed before the request was admitted";
+                    r->t_done = Clock::now();
+                    r->done = true;
+                }
+                s->queue.clear();
+                s->cv_done.notify_all();
+            }
+            s->n_queued = int(s->queue.size());
+            if (s->stop && s->active.empty()) return;
+        }
+        bool progress = false;
+        // completions (in stream order within each lane)
+        for (Lane& ln : s->lanes) {
+            while (!ln.flight.empty()) {
+                Flight f = ln.flight.front();
+                const cudaError_t q = cudaEventQuery(f.ev);
+                if (q == cudaErrorNotReady) break;
+                if (q != cudaSuccess) {
+                    cudaGetLastError();
+                    fail_all(s, std::string("device error: ") + cudaGetErrorString(q));
+                    return;
+                }
+                ln.flight.pop_front();
+                s->ev_pool.push_back(f.ev);
+                if (f.last) finish(s, f.r);
+                progress = true;
+            }
+        }
+        // admission, first come first served
+        while (!s->queue.empty() && admit(s, s->queue.front()) != Admit::kNoRoom) {
+            s->queue.pop_front();
+            progress = true;
+        }
+        s->n_queued = int(s->queue.size());
+        // issue: per lane, the admitted request with the least remaining work
+        for (size_t li = 0; li < s->lanes.size(); ++li) {
+            Lane& ln = s->lanes[li];
+            while (int(ln.flight.size()) < depth) {
+                Request* best = nullptr;
+                for (Request* r : s->active)
+                    if (r->lane == int(li) && r->next < r->chunks.size() &&
+                        (!best || r->remaining < best->remaining))
+                        best = r;
+                if (!best) break;
+                if (!issue(s, best)) {
+                    cudaGetLastError();
+                    fail_all(s, std::string("launch failed: ") + xs_last_error());
+                    return;
+                }
+                progress = true;
+            }
+        }
+        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int xs_server_create(int device, const xs_server_config* cfg, xs_server** out) {
+    if (!out) return sfail(XS_ERR_INVALID, "xs_server_create: out is NULL");
+    *out = nullptr;
+    xs_server_config c{};
+    if (cfg) c = *cfg;
+    if (c.lanes <= 0) c.lanes = 4;
+    if (c.depth <= 0) c.depth = 2;
+    if (!(c.chunk_pairs > 0.0)) c.chunk_pairs = 4.0e9;
+    if (c.chunk_lines == 0) c.chunk_lines = size_t(1) << 22;
+    if (c.host_budget == 0) c.host_budget = size_t(1) << 30;
+    if (c.lanes > 16 || c.depth > 8) return sfail(XS_ERR_INVALID, "xs_server_create: lanes <= 16, depth <= 8");
+    auto* s = new xs_server();
+    s->device = device;
+    s->cfg = c;
+    s->mols.reserve(kMaxMolecules);
+    DevGuard dg(device);
+    // lanes: a stream and an engine each, scratch sized for the largest chunk
+    xs_options o{};
+    o.profile = XS_VOIGT;
+    o.precision = XS_FP64;
+    size_t scratch = xs_scratch_bytes_needed(&o, 1, c.chunk_lines);
+    o.precision = XS_MIXED;
+    scratch = std::max(scratch, xs_scratch_bytes_needed(&o, 1, c.chunk_lines));
+    for (int k = 0; k < c.lanes; ++k) {
+        Lane ln;
+        int rc = xs_engine_create(device, &ln.eng);
+        if (rc == XS_OK && cudaStreamCreateWithFlags(&ln.st, cudaStreamNonBlocking) != cudaSuccess)
+            rc = sfail(XS_ERR_CUDA, "cudaStreamCreate");
+        if (rc == XS_OK) rc = xs_engine_set_stream(ln.eng, ln.st);
+        if (rc == XS_OK) rc = xs::engine_reserve(ln.eng, scratch);
+        if (rc != XS_OK) {
+            if (ln.eng) xs_engine_destroy(ln.eng);
+            if (ln.st) cudaStreamDestroy(ln.st);
+            for (Lane& l : s->lanes) {
+                xs_engine_destroy(l.eng);
+                cudaStreamDestroy(l.st);
+            }
+            delete s;
+            return rc;
+        }
+        s->lanes.push_back(ln);
+    }
+    s->resident = scratch * size_t(c.lanes) + (size_t(4) << 20) * size_t(c.lanes);
+    if (c.device_budget == 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        s->cfg.device_budget = fr > (size_t(2) << 30) ? fr - (size_t(2) << 30) : fr / 2;
+        s->cfg.device_budget += s->resident;
+    }
+    if (s->resident > s->cfg.device_budget) {
+        for (Lane& l : s->lanes) {
+            xs_engine_destroy(l.eng);
+            cudaStreamDestroy(l.st);
+        }
+        delete s;
+        return sfail(XS_ERR_NOMEM, "xs_server_create: the lanes' scratch alone exceeds device_budget");
+    }
+    // keep freed request memory in the pool instead of returning it
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        unsigned long long thr = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+    if (!s->arena.init(c.host_budget)) {
+        for (Lane& l : s->lanes) {
+            xs_engine_destroy(l.eng);
+            cudaStreamDestroy(l.st);
+        }
+        delete s;
+        return sfail(XS_ERR_NOMEM, "xs_server_create: pinned host arena");
+    }
+    s->worker = std::thread(scheduler, s);
+    *out = s;
+    return XS_OK;
+}
+
+int xs_server_destroy(xs_server* s) {
+    if (!s) return XS_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    DevGuard dg(s->device);
+    for (Lane& l : s->lanes) {
+        cudaStreamSynchronize(l.st);
+        for (Flight& f : l.flight) cudaEventDestroy(f.ev);
+        xs_engine_destroy(l.eng);
+        cudaStreamDestroy(l.st);
+    }
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    for (Molecule& m : s->mols) {
+        cudaFree(m.nu);
+        cudaFree(m.e);
+        cudaFree(m.a);
+        cudaFree(m.g);
+        cudaFree(m.nx);
+        cudaFree(m.gns);
+    }
+    for (auto& kv : s->all) delete kv.second;
+    s->arena.release();
+    delete s;
+    return XS_OK;
+}
+
+int xs_server_add_molecule(xs_server* s, const double* nu, const double* energies,
+                           const double* aif, const int* gns, const double* gamma,
+                           const double* n, size_t count, double mean_mass, double ref_temp,
+                           int* molecule_id) {
+    if (!s || !nu || !energies || !aif || !gns || !gamma || !n || !molecule_id || count == 0)
+        return sfail(XS_ERR_INVALID, "xs_server_add_molecule: NULL argument or no lines");
+    if (!(mean_mass > 0.0) || !(ref_temp > 0.0))
+        return sfail(XS_ERR_INVALID, "xs_server_add_molecule: mass and reference temperature must be > 0");
+    for (size_t i = 1; i < count; ++i)
+        if (nu[i] < nu[i - 1])
+            return sfail(XS_ERR_UNSORTED, "xs_server_add_molecule: line centres must be ascending");
+    const size_t bytes = count * (5 * sizeof(double) + sizeof(int));
+    DevGuard dg(s->device);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->resident + s->dev_requests + bytes > s->cfg.device_budget)
+        return sfail(XS_ERR_NOMEM, "xs_server_add_molecule: over the device budget");
+    if (s->mols.size() >= kMaxMolecules)
+        return sfail(XS_ERR_INVALID, "xs_server_add_molecule: at most 64 molecules per server");
+    Molecule m;
+    m.n = count;
+    m.mass = mean_mass;
+    m.ref_temp = ref_temp;
+    m.bytes = bytes;
+    cudaError_t err = cudaSuccess;
+    auto put = [&](double** dst, const double* src) {
+        if (err == cudaSuccess) err = cudaMalloc(dst, count * sizeof(double));
+        if (err == cudaSuccess) err = cudaMemcpy(*dst, src, count * sizeof(double), cudaMemcpyHostToDevice);
+    };
+    put(&m.nu, nu);
+    put(&m.e, energies);
+    put(&m.a, aif);
+    put(&m.g, gamma);
+    put(&m.nx, n);
+    if (err == cudaSuccess) err = cudaMalloc(&m.gns, count * sizeof(int));
+    if (err == cudaSuccess) err = cudaMemcpy(m.gns, gns, count * sizeof(int), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(m.nu);
+        cudaFree(m.e);
+        cudaFree(m.a);
+        cudaFree(m.g);
+        cudaFree(m.nx);
+        cudaFree(m.gns);
+        return sfail(err == cudaErrorMemoryAllocation ? XS_ERR_NOMEM : XS_ERR_CUDA,
+                     std::string("xs_server_add_molecule: ") + cudaGetErrorString(err));
+    }
+    m.h_nu.assign(nu, nu + count);
+    m.h_cum.resize(count + 1);
+    m.h_cum[0] = 0.0;
+    for (size_t i = 0; i < count; ++i) m.h_cum[i + 1] = m.h_cum[i] + nu[i];
+    s->resident += bytes;
+    *molecule_id = int(s->mols.size());
+    s->mols.push_back(std::move(m));
+    return XS_OK;
+}
+
+int xs_server_submit(xs_server* s, const xs_request* q, unsigned long long* request_id) {
+    if (!s || !q || !request_id) return sfail(XS_ERR_INVALID, "xs_server_submit: NULL argument");
+    const auto t0 = Clock::now();
+    *request_id = 0;
+    int nmol;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (!s->fatal.empty()) return sfail(XS_ERR_CUDA, "server stopped: " + s->fatal);
+        nmol = int(s->mols.size());
+    }
+    if (q->molecule < 0 || q->molecule >= nmol) return sfail(XS_ERR_INVALID, "xs_server_submit: no such molecule");
+    if (q->profile != XS_VOIGT && q->profile != XS_DOPPLER)
+        return sfail(XS_ERR_UNSUPPORTED, "xs_server_submit: profile must be VOIGT or DOPPLER");
+    if (q->precision != XS_FP64 && q->precision != XS_MIXED)
+        return sfail(XS_ERR_INVALID, "xs_server_submit: precision");
+    if (!(q->temperature > 0.0) || !(q->partition > 0.0) || !(q->df > 0.0) || q->npoints < 1 ||
+        !(q->pressure > 0.0))
+        return sfail(XS_ERR_INVALID, "xs_server_submit: T, Q, P and df must be > 0, npoints >= 1");
+    auto* r = new Request();
+    r->q = *q;
+    const Molecule& m = s->mols[size_t(q->molecule)];
+    r->opt.profile = q->profile;
+    r->opt.convention = XS_CONV_GPU;
+    r->opt.precision = q->precision;
+    r->opt.cpu_threads = 1;
+    r->opt.mean_mass = m.mass;
+    r->opt.ref_temp = m.ref_temp;
+    r->opt.half_width = 0.1;
+    r->opt.dfreq = q->df;
+    r->cond.temperature = q->temperature;
+    r->cond.partition = q->partition;
+    r->cond.pressure = q->pressure;
+    r->cond.gamma_scale = q->pressure;
+    r->cond.cut = q->cut;
+    const double cut = q->cut > 0.0 ? q->cut
+                                     : (q->profile == XS_VOIGT ? std::fmin(25.0 * q->pressure, 100.0) : 100.0);
+    plan_chunks(m.index(), q->f0, q->df, q->npoints, cut, s->cfg.chunk_pairs, s->cfg.chunk_lines, r->chunks);
+    for (const ChunkPlan& c : r->chunks) {
+        if (c.l1 - c.l0 > s->cfg.chunk_lines) {
+            delete r;
+            return sfail(XS_ERR_NOMEM, "xs_server_submit: a single 256-point tile needs more lines "
+                                       "than chunk_lines");
+        }
+        r->pairs += c.pairs;
+    }
+    r->remaining = r->pairs;
+    r->lines = m.index().upper(q->f0 + double(q->npoints - 1) * q->df + cut) -
+               m.index().lower(q->f0 - cut);
+    r->dev_bytes = request_device_bytes(*q);
+    if (s->resident + r->dev_bytes > s->cfg.device_budget ||
+        sizeof(double) * size_t(q->npoints) + 256 > s->arena.size()) {
+        delete r;
+        return sfail(XS_ERR_NOMEM, "xs_server_submit: the request alone exceeds the memory budget");
+    }
+    r->t_submit = t0;
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->id = s->next_id++;
+    s->all[r->id] = r;
+    s->incoming.push_back(r);
+    s->cv_work.notify_all();
+    *request_id = r->id;
+    return XS_OK;
+}
+
+int xs_server_wait(xs_server* s, unsigned long long id, double* out, int npoints,
+                   xs_request_info* info, int timeout_ms) {
+    if (!s) return sfail(XS_ERR_INVALID, "xs_server_wait: NULL server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return sfail(XS_ERR_INVALID, "xs_server_wait: unknown request id");
+    Request* r = it->second;
+    auto ready = [&] { return r->done; };
+    if (timeout_ms < 0)
+        s->cv_done.wait(lk, ready);
+    else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+        return sfail(XS_ERR_TIMEOUT, "xs_server_wait: not finished yet");
+    if (info) {
+        info->status = r->status;
+        info->latency_ms = ms_between(r->t_submit, r->t_done);
+        info->queue_ms = r->t_admit.time_since_epoch().count() ? ms_between(r->t_submit, r->t_admit) : 0.0;
+        info->run_ms = r->t_admit.time_since_epoch().count() ? ms_between(r->t_admit, r->t_done) : 0.0;
+        info->chunks = int(r->chunks.size());
+        info->line_evals = r->pairs;
+        info->lines = r->lines;
+    }
+    int rc = r->status;
+    std::string err = r->error;
+    if (rc == XS_OK && out) {
+        if (npoints != r->q.npoints) {
+            rc = XS_ERR_INVALID;
+            err = "xs_server_wait: npoints differs from the request's";
+        } else {
+            std::memcpy(out, s->arena.at(r->host_off), sizeof(double) * size_t(npoints));
+        }
+    }
+    if (r->host_off != SIZE_MAX) s->arena.free(r->host_off, r->host_bytes);
+    s->all.erase(it);
+    delete r;
+    if (rc != XS_OK) return sfail(rc, err.empty() ? "request failed" : err);
+    return XS_OK;
+}
+
+int xs_server_pending(xs_server* s, int* queued, int* active) {
+    if (!s) return sfail(XS_ERR_INVALID, "xs_server_pending: NULL server");
+    if (queued) *queued = s->n_queued;
+    if (active) *active = s->n_active;
+    return XS_OK;
+}
+
+int xs_plan_chunks(const double* nu, size_t n, double f0, double df, int npoints, double cut,
+                   double max_pairs, size_t max_lines, int cap, int* start, int* points,
+                   size_t* l0, size_t* l1, double* pairs, int* nchunks) {
+    if ((!nu && n) || !nchunks || npoints < 1 || !(df > 0.0) || !(cut > 0.0) || !(max_pairs > 0.0))
+        return sfail(XS_ERR_INVALID, "xs_plan_chunks: bad arguments");
+    for (size_t i = 1; i < n; ++i)
+        if (nu[i] < nu[i - 1]) return sfail(XS_ERR_UNSORTED, "xs_plan_chunks: nu must be ascending");
+    std::vector<double> cum(n + 1, 0.0);
+    for (size_t i = 0; i < n; ++i) cum[i + 1] = cum[i] + nu[i];
+    LineIndex L;
+    L.nu = nu;
+    L.cum = cum.data();
+    L.n = n;
+    std::vector<ChunkPlan> plan;
+    plan_chunks(L, f0, df, npoints, cut, max_pairs, max_lines ? max_lines : SIZE_MAX, plan);
+    *nchunks = int(plan.size());
+    if (int(plan.size()) > cap) return sfail(XS_ERR_INVALID, "xs_plan_chunks: more chunks than cap");
+    for (size_t k = 0; k < plan.size(); ++k) {
+        if (start) start[k] = plan[k].start;
+        if (points) points[k] = plan[k].points;
+        if (l0) l0[k] = plan[k].l0;
+        if (l1) l1[k] = plan[k].l1;
+        if (pairs) pairs[k] = plan[k].pairs;
+    }
+    return XS_OK;
+}
+
+}  // extern "C"

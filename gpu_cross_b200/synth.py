@@ -163,3 +163,44 @@ def voigt_sweep_workload(n_lines: int = 10_000_000, grid_points: int = 75_000):
                          pressure_atm=1.0)
     grid = Grid(500.0, 8000.0, grid_points)
     return lines, grid, sweep_conditions(), dict(mean_mass=17.03, ref_temp=296.0)
+
+
+# Serving: three resident molecules and a seeded Poisson request stream.
+SERVE_MOLECULES = ((1_000_000, 18.02), (10_000_000, 30.01), (100_000_000, 16.04))
+
+
+def serving_molecules(scale: float = 1.0):
+    """[(LineList, mass)] for the three served molecules: 1e6, 1e7 and 1e8
+    lines (times scale) with nu ~ U(0, 12000) and the single-point list's
+    other statistics; gamma per atm at 296 K."""
+    out = []
+    for k, (n, mass) in enumerate(SERVE_MOLECULES):
+        m = max(1000, int(n * scale))
+        out.append((random_lines(m, 0.0, 12000.0, 2500.0, 1e-6, 1e2, seed=1005 + 10 * k,
+                                 pressure_atm=1.0), mass))
+    return out
+
+
+def serving_trace(rate: float = 200.0, duration_s: float = 10.0, seed: int = 1005,
+                  n_molecules: int = 3):
+    """Poisson arrivals (mean `rate` per second) over duration_s; each request:
+    molecule uniform, T ~ U(200, 3000) K, P ~ logU(1e-5, 100) bar,
+    Doppler or Voigt (1/2 each), span ~ U(100, 5000) cm-1 inside 0-12000,
+    resolution df ~ logU(0.01, 1) cm-1, cut 25 cm-1, Q = partition_poly(T)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = 0.0
+    out = []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration_s:
+            break
+        span = rng.uniform(100.0, 5000.0)
+        df = math.exp(rng.uniform(math.log(0.01), math.log(1.0)))
+        f0 = rng.uniform(0.0, 12000.0 - span)
+        temp = rng.uniform(200.0, 3000.0)
+        p_bar = math.exp(rng.uniform(math.log(1e-5), math.log(100.0)))
+        out.append(dict(t=t, molecule=int(rng.integers(0, n_molecules)),
+                        voigt=bool(rng.random() < 0.5), temperature=temp,
+                        partition=partition_poly(temp), pressure=p_bar * BAR_TO_ATM,
+                        f0=f0, df=df, npoints=max(1, int(round(span / df))), cut=25.0))
+    return out

@@ -251,6 +251,77 @@ int xs_manager_cleanup(xs_manager* m);
 int xs_manager_ready_for_work(xs_manager* m, int* ready);
 int xs_manager_get_ntrans(xs_manager* m, size_t* ntrans);
 
+/* ---- 4. server level: a continuous-batching request loop ----------------- */
+/* No counterpart in the reference, which computes one .inp job per process.
+ * Line lists stay resident in device memory; requests (molecule, T, Q(T), P,
+ * profile, grid) arrive at any time from any thread and are admitted while
+ * their memory fits the budgets.  Each request's grid is split into chunks
+ * of whole 256-point tiles with bounded work; a scheduler thread interleaves
+ * the chunks of all admitted requests over several streams (the request
+ * with the least remaining work first), so a request that arrives while a
+ * large one runs does not wait for all of it.  A request's chunks depend
+ * only on the request, so its result is the same alone and in any mix. */
+typedef struct xs_server xs_server;
+
+typedef struct {
+    size_t device_budget; /* bytes of device memory for molecules, lane scratch
+                             and admitted requests (0 = free memory - 2 GiB) */
+    size_t host_budget;   /* pinned host bytes for results (0 = 1 GiB) */
+    int lanes;            /* streams, each with its own engine (0 = 4) */
+    int depth;            /* chunks in flight per lane (0 = 2) */
+    double chunk_pairs;   /* target line-evals per chunk (0 = 4e9) */
+    size_t chunk_lines;   /* most lines in one chunk's slice (0 = 2^22) */
+} xs_server_config;
+
+typedef struct {
+    int molecule;       /* id from xs_server_add_molecule */
+    int profile;        /* XS_VOIGT or XS_DOPPLER */
+    int precision;      /* XS_FP64 or XS_MIXED */
+    double temperature; /* K */
+    double partition;   /* Q(T) */
+    double pressure;    /* atm: multiplies the molecule's gamma (given per atm)
+                           and, when cut <= 0, sets the reference cut rule */
+    double cut;         /* window half width in cm-1; <= 0: min(25 P, 100) for
+                           Voigt, 100 for Doppler */
+    double f0, df;      /* grid f_i = f0 + i*df ... */
+    int npoints;        /* ... for i < npoints */
+} xs_request;
+
+typedef struct {
+    int status;         /* XS_OK or the request's error */
+    double latency_ms;  /* submit -> result in host memory */
+    double queue_ms;    /* submit -> admitted */
+    double run_ms;      /* admitted -> result in host memory */
+    int chunks;
+    double line_evals;  /* sum of window overlaps / df (an estimate) */
+    size_t lines;       /* lines within the grid +/- cut */
+} xs_request_info;
+
+int xs_server_create(int device, const xs_server_config* cfg, xs_server** out);
+/* Finishes the requests already submitted, then frees everything. */
+int xs_server_destroy(xs_server* s);
+/* Copies a nu-ascending line list to the device (gamma per atm at ref_temp);
+ * at most 64 molecules. */
+int xs_server_add_molecule(xs_server* s, const double* nu, const double* energies,
+                           const double* aif, const int* gns, const double* gamma,
+                           const double* n, size_t count, double mean_mass, double ref_temp,
+                           int* molecule_id);
+/* Non-blocking.  XS_ERR_NOMEM when the request alone exceeds a budget. */
+int xs_server_submit(xs_server* s, const xs_request* r, unsigned long long* request_id);
+/* Blocks until the request is done (timeout_ms < 0: no limit; on timeout
+ * XS_ERR_TIMEOUT and the request stays), copies its npoints results to out
+ * (may be NULL), fills info (may be NULL) and forgets the request. */
+int xs_server_wait(xs_server* s, unsigned long long request_id, double* out, int npoints,
+                   xs_request_info* info, int timeout_ms);
+int xs_server_pending(xs_server* s, int* queued, int* active);
+/* The server's chunk planner, on host arrays (no device needed): chunks of
+ * whole 256-point tiles, each with at most max_pairs estimated line-evals
+ * (unless one tile alone has more) and max_lines lines (0 = no limit).
+ * Fills up to cap entries; *nchunks gets the count. */
+int xs_plan_chunks(const double* nu, size_t n, double f0, double df, int npoints, double cut,
+                   double max_pairs, size_t max_lines, int cap, int* start, int* points,
+                   size_t* l0, size_t* l1, double* pairs, int* nchunks);
+
 #ifdef __cplusplus
 }
 #endif

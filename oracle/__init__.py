@@ -82,10 +82,18 @@ def _arrs(lines):
 
 
 def gpu_convention(profile: int, freq: np.ndarray, intens: np.ndarray, lines, cond: dict,
-                   dfreq: float, points: int | None = None, start_idx: int = 0) -> np.ndarray:
+                   dfreq: float, points: int | None = None, start_idx: int = 0,
+                   cut: float | None = None) -> np.ndarray:
     """The reference GpuManager path (cross_kernal.cu block kernels), restated
-    in C.  Returns a new grid = intens + contributions."""
+    in C.  Returns a new grid = intens + contributions.  cut: window half
+    width in place of the reference rule (Voigt and Doppler)."""
     lib = oracle_lib()
+    if cut is not None:
+        lib.oracle_set_cut(ctypes.c_double(cut))
+        try:
+            return gpu_convention(profile, freq, intens, lines, cond, dfreq, points, start_idx)
+        finally:
+            lib.oracle_set_cut(ctypes.c_double(-1.0))
     out = np.array(intens, dtype=np.float64, copy=True)
     fr = np.ascontiguousarray(freq, dtype=np.float64)
     pts = len(fr) - start_idx if points is None else points

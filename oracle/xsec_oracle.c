@@ -151,11 +151,17 @@ static long lower_bound_d(const double* nu, long n, double v) {
  * For ascending nu the lines a thread evaluates are exactly its stride
  * members inside [-cut, cut]; the loop below visits those directly.
  * kind: 2 Voigt, 1 Doppler. */
+/* Window half width override for the GPU convention (cut > 0), as the
+ * engine's xs_condition.cut; <= 0 restores the reference rule. */
+static double g_cut_override = -1.0;
+void oracle_set_cut(double cut) { g_cut_override = cut; }
+
 static void gpu_steptwo(int kind, const oracle_consts* c, const double* freq, double* intens,
                         int points, int start_idx, long n, const double* nu, const double* s,
                         const double* gl, int nthr) {
     double dpw = sqrt(2.0 * O_BOLTZ * c->temperature * O_NA / (c->mean_mass)) / O_VELLGT;
     double cut = (kind == 2) ? fmin(25.0 * c->pressure, 100.0) : O_DOPPLER_CUTOFF;
+    if (g_cut_override > 0.0) cut = g_cut_override;
     double x0d = c->dfreq * 0.5;
     int sorted = is_sorted_nu(n, nu);
     double* part = (double*)malloc(sizeof(double) * (size_t)nthr);
