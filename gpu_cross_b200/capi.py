@@ -45,7 +45,7 @@ class Options(ctypes.Structure):
                 ("mean_mass", ctypes.c_double), ("ref_temp", ctypes.c_double),
                 ("half_width", ctypes.c_double), ("dfreq", ctypes.c_double),
                 ("points_per_thread", ctypes.c_int), ("warps_per_block", ctypes.c_int),
-                ("conditions_per_warp", ctypes.c_int)]
+                ("conditions_per_warp", ctypes.c_int), ("line_splits", ctypes.c_int)]
 
 
 class Lines(ctypes.Structure):
@@ -275,9 +275,10 @@ def make_grid(freq, start_idx: int = 0, points: int | None = None) -> GridC:
 def make_options(profile: int, dfreq: float, mean_mass: float, convention: int = CONV_GPU,
                  precision: int = FP64, cpu_threads: int = 1, ref_temp: float = 296.0,
                  half_width: float = 0.1, points_per_thread: int = 0,
-                 warps_per_block: int = 0, conditions_per_warp: int = 0) -> Options:
+                 warps_per_block: int = 0, conditions_per_warp: int = 0,
+                 line_splits: int = 0) -> Options:
     return Options(profile, convention, precision, cpu_threads, mean_mass, ref_temp, half_width,
-                   dfreq, points_per_thread, warps_per_block, conditions_per_warp)
+                   dfreq, points_per_thread, warps_per_block, conditions_per_warp, line_splits)
 
 
 def make_condition(temperature: float, partition: float, pressure: float = 1.0,

@@ -354,6 +354,8 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
     }
     const int CG = C > 1 ? C : 0;
+    if (opt->line_splits < 0 || opt->line_splits > kMaxSplits)
+        return fail(XS_ERR_INVALID, "line_splits must be 0 (automatic) .. 64");
 
     std::lock_guard<std::mutex> lk(e->mu);
     DeviceGuard dg(e->device);
@@ -361,7 +363,40 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     // Scratch layout for one group of conditions.
     const int group = ncond < kMaxCond ? ncond : kMaxCond;
     const ScratchPlan plan = plan_scratch(kind, mixed, size_t(n), group, 0, CG);
-    const size_t need = plan.need;
+    int occ = CG ? steptwo_mc_blocks_per_sm(mixed, CG, W)
+                 : steptwo_blocks_per_sm(kind, opt->convention, mixed, P, W);
+    if (occ < 1) occ = 1;
+
+    // Line splits.  A launch with fewer work items than resident warps
+    // (short or coarse grids over many lines) would leave most of the GPU
+    // idle while each warp walks a long line list; then each tile's lines
+    // are split into parts taken by different warps -- enough for about two
+    // waves, at least ~128 lines per part, the parts' buffer within
+    // kMaxPartBytes.  The count depends only on the call's sizes and the SM
+    // count.
+    const int tile_pts = CG ? 32 : 32 * P;
+    const int tiles = (grid->points + tile_pts - 1) / tile_pts;
+    int S = opt->line_splits;
+    if (ov && ov->scratch) S = 1;  // a fixed caller scratch holds no parts
+    if (S == 0) {
+        const long items = long(tiles) * (CG ? group / CG : group);
+        const long warps = long(occ) * W * e->num_sms;
+        S = 1;
+        if (items < warps) {
+            double cutmax = 0.0;
+            for (int c = 0; c < ncond; ++c) cutmax = std::fmax(cutmax, make_cond(*opt, conds[c]).cut);
+            const double span = double(grid->points) * opt->dfreq + 2.0 * cutmax;
+            const double lpt = double(n) * (double(tile_pts) * opt->dfreq + 2.0 * cutmax) / span;
+            long want = (2 * warps + items - 1) / items;
+            want = std::min<long>(want, long(lpt / 128.0));
+            const long cap = long(kMaxPartBytes / (sizeof(double) * size_t(group) * size_t(grid->points)));
+            want = std::min<long>(want, std::min<long>(cap, kMaxSplits));
+            if (want > 1) S = int(want);
+        }
+    }
+    const size_t part_off = (plan.need + 255) & ~size_t(255);
+    const size_t need = S > 1 ? part_off + sizeof(double) * size_t(S) * size_t(group) * size_t(grid->points)
+                              : plan.need;
 
     void* scratch = nullptr;
     unsigned* words = e->d_words;
@@ -468,8 +503,11 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         sa.out_stride = out_stride;
         sa.G = G;
         sa.tiles_per_cond = (grid->points + 32 * P - 1) / (32 * P);
-        sa.n_items = sa.tiles_per_cond * nc;
+        sa.n_items = sa.tiles_per_cond * nc * S;
         sa.counter = words + 1;
+        sa.splits = S;
+        sa.part = S > 1 ? reinterpret_cast<double*>(base + part_off) : nullptr;
+        sa.part_stride = size_t(grid->points);
         sa.x0 = pa.x0;
         sa.xg = pa.xg;
         sa.x0g = pa.x0g;
@@ -479,16 +517,15 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
             sa.lsh = pa.lsh;
             sa.group = CG;
             sa.tiles_per_cond = (grid->points + 31) / 32;
-            sa.n_items = sa.tiles_per_cond * (nc / CG);
+            sa.n_items = sa.tiles_per_cond * (nc / CG) * S;
         }
-        int occ = CG ? steptwo_mc_blocks_per_sm(mixed, CG, W)
-                    : steptwo_blocks_per_sm(kind, opt->convention, mixed, P, W);
-        if (occ < 1) occ = 1;
         const long want = (long(sa.n_items) + W - 1) / W;
         const int blocks = int(std::min<long>(want, long(occ) * e->num_sms));
         err = CG ? launch_steptwo_mc(mixed, CG, W, blocks, sa, st)
                 : launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step two launch");
+        err = launch_reduce_splits(sa, nc, st);
+        if (err != cudaSuccess) return cuda_fail(err, "split reduction launch");
         if (timing && c0 + nc >= ncond) {
             cudaEventRecordWithFlags(e->ev[2], st, ev_flags);
             e->timed = true;

@@ -37,6 +37,8 @@ constexpr unsigned kErrUnsorted = 1u;
 constexpr unsigned kErrGrid = 2u;
 
 constexpr int kMaxCond = 64;  // conditions per launch (the sweep uses 40)
+constexpr int kMaxSplits = 64;                      // line splits per tile
+constexpr size_t kMaxPartBytes = size_t(64) << 20;  // automatic splits' part buffer
 
 // Per-condition constants, computed on the host exactly as the selected
 // reference backend computes them (GPUManager.cpp:24-47 for the GPU
@@ -173,6 +175,13 @@ struct StepArgs {
     int n_items;
     unsigned* counter;
     double x0, xg, x0g;  // Doppler / Gaussian constants
+    // Line splits: with splits > 1 every tile is taken by `splits` work
+    // items, each over one contiguous part of the tile's lines; item s
+    // stores its sums to part[(c * splits + s) * part_stride + j - G.start]
+    // and k_reduce_splits adds the parts, in order, to out.
+    int splits;
+    double* part;
+    size_t part_stride;
 };
 
 // Kernel launchers (xs_kernels.cu).  All asynchronous on `stream`.
@@ -181,6 +190,8 @@ cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaS
 // P = points per thread (1, 2, 4, 8), warps per block (4 or 8).
 cudaError_t launch_steptwo(int kind, int conv, bool mixed, int P, int warps, int blocks,
                            const StepArgs& a, cudaStream_t stream);
+// out[c][G.start + j] += sum over s of part[(c * splits + s) * stride + j].
+cudaError_t launch_reduce_splits(const StepArgs& a, int ncond_out, cudaStream_t stream);
 // Resident blocks per SM for a step-two configuration.
 int steptwo_blocks_per_sm(int kind, int conv, bool mixed, int P, int warps);
 size_t record_bytes(int kind, bool mixed);

@@ -428,20 +428,44 @@ __device__ __forceinline__ void stage(REC* dst, const REC* src, int cnt, int lan
 }
 
 struct WorkItem {
-    int c, t0, t1;
+    int c, t0, t1, s;
 };
 
+// Items are (condition, tile, split), splits innermost: the parts of one
+// tile run side by side and share its records in L2.
 __device__ __forceinline__ bool next_item(const StepArgs& a, int P, int lane, WorkItem& w) {
     int item = 0;
     if (lane == 0) item = int(atomicAdd(a.counter, 1u));
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= a.n_items) return false;
-    w.c = item / a.tiles_per_cond;
-    const int tile = item - w.c * a.tiles_per_cond;
+    const int per_cond = a.tiles_per_cond * a.splits;
+    w.c = item / per_cond;
+    const int rem = item - w.c * per_cond;
+    const int tile = rem / a.splits;
+    w.s = rem - tile * a.splits;
     w.t0 = a.G.start + tile * 32 * P;
     const int end = a.G.start + a.G.points;
     w.t1 = w.t0 + 32 * P < end ? w.t0 + 32 * P : end;
     return true;
+}
+
+// The part [La, Lb) of a tile's lines that split s of `splits` takes.
+__device__ __forceinline__ void split_range(int splits, int s, long& La, long& Lb) {
+    if (splits <= 1) return;
+    const int nl = int(Lb - La);  // lines per tile < 2^31 (the engine limit)
+    const int per = (nl + splits - 1) / splits;
+    const int a0 = min(per * s, nl), b0 = min(per * (s + 1), nl);
+    Lb = La + b0;
+    La = La + a0;
+}
+
+// Where item (c, s) puts the sum of grid point j: added to out, or stored to
+// its part when the tile is split.
+__device__ __forceinline__ void put_result(const StepArgs& a, int c, int s, int j, double v) {
+    if (a.splits <= 1)
+        a.out[size_t(c) * a.out_stride + size_t(j)] += v;
+    else
+        a.part[(size_t(c) * a.splits + s) * a.part_stride + size_t(j - a.G.start)] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -645,13 +669,15 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
         const int* mi = a.mi;
         const int kc = a.kc[w.c];
         const int t0 = w.t0, t1 = w.t1, tl = t1 - 1;
-        const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
-        const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
+        long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
+        long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
         const long fs = warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; });
         const long Cb = warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; });
         const long fe = Cb > fs ? Cb : fs;
         const long E = warp_lower_bound(fs, fe, lane, [&](long i) { return mi[i] >= t0 - kc; });
         const long Fc = warp_lower_bound(E, fe, lane, [&](long i) { return mi[i] > tl + kc; });
+        // the runs above stay as found; the groups below clip them to the part
+        split_range(a.splits, w.s, La, Lb);
         const REC* recs = recs_all + cbase;
 
         int jj[P];
@@ -932,12 +958,11 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             }
             __syncwarp();
         }
-        double* out = a.out + size_t(w.c) * a.out_stride;
 #pragma unroll
         for (int p = 0; p < P; ++p) {
             if (jj[p] < t1) {
                 const double v = MIXED ? double(sumf[p]) - double(cmpf[p]) : accd[p];
-                out[jj[p]] += v;
+                put_result(a, w.c, w.s, jj[p], v);
             }
         }
     }
@@ -993,8 +1018,10 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
         if (lane == 0) item = int(atomicAdd(a.counter, 1u));
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= a.n_items) break;
-        const int cg = item / a.tiles_per_cond;
-        const int tile = item - cg * a.tiles_per_cond;
+        const int per_cond = a.tiles_per_cond * a.splits;
+        const int cg = item / per_cond;
+        const int tile = (item - cg * per_cond) / a.splits;
+        const int split = item - cg * per_cond - tile * a.splits;
         const int t0 = a.G.start + tile * 32;
         const int end = a.G.start + a.G.points;
         const int t1 = t0 + 32 < end ? t0 + 32 : end;
@@ -1006,13 +1033,14 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
         int kc = 0;
 #pragma unroll
         for (int c = 0; c < C; ++c) kc = max(kc, a.kc[cg * C + c]);
-        const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
-        const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
+        long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
+        long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
         const long fs = warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; });
         const long Cb = warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; });
         const long fe = Cb > fs ? Cb : fs;
         const long E = warp_lower_bound(fs, fe, lane, [&](long i) { return mi[i] >= t0 - kc; });
         const long Fc = warp_lower_bound(E, fe, lane, [&](long i) { return mi[i] > tl + kc; });
+        split_range(a.splits, split, La, Lb);
         const LS* lsh = reinterpret_cast<const LS*>(a.lsh) + gbase;
         const CR* crec = reinterpret_cast<const CR*>(a.rec) + gbase * C;
 
@@ -1114,7 +1142,11 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
                     for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], T(1), c);
                 }
             }
-            // core lines (window covers the row) and partial lines
+            // core-candidate lines (window covers the row) and partial lines.
+            // Per condition: when its core band misses the row (the usual
+            // case for partial lines, whose centres lie about a cut away),
+            // region I with the window as a lane mask; otherwise the
+            // lane-by-lane core path.
             for (int t = a0; t < e1; ++t) {
                 if (t == a1) t = b1;
                 if (t == c1) t = d1;
@@ -1122,10 +1154,28 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
                 const LS s = SL[t];
                 const bool full = (t >= b1 && t < c1);
                 const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
-                const int mline = mi[gb + t];
+                const T mask = in ? T(1) : T(0);
+                int mline;
+                if constexpr (MIXED) mline = int(s.m);  // exact below 2^24; "whole" lines have unbounded bands
+                else mline = mi[gb + t];
+                bool any_core = false;
 #pragma unroll
-                for (int c = 0; c < C; ++c) core_cond(s, SC[t * C + c], mline, in, c);
-                while (qn >= 32) qn = core_queue_flush<C, MIXED>(cq, qn, 32, lane);
+                for (int c = 0; c < C; ++c) {
+                    const CR& r = SC[t * C + c];
+                    bool hit = false;
+                    if (r.core != -1) {
+                        const int aa = r.core & 0xffff, bb = (r.core >> 16) & 0xffff;
+                        hit = (aa == 0x7fff || mline - aa <= tl) && (bb == 0x7fff || mline + bb >= t0);
+                    }
+                    if (!hit) {
+                        region1(offset(s, r), r, mask, c);
+                    } else {
+                        core_cond(s, r, mline, in, c);
+                        any_core = true;
+                    }
+                }
+                if (any_core)
+                    while (qn >= 32) qn = core_queue_flush<C, MIXED>(cq, qn, 32, lane);
             }
             if (MIXED) {
                 if (qn > 0) qn = core_queue_flush<C, MIXED>(cq, qn, qn, lane);
@@ -1155,7 +1205,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 const double v = MIXED ? double(sumf[c]) - double(cmpf[c]) : accd[c];
-                a.out[size_t(cg * C + c) * a.out_stride + size_t(jj)] += v;
+                put_result(a, cg * C + c, split, jj, v);
             }
         }
     }
@@ -1179,8 +1229,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_erf(StepArgs a) {
         const int* whi = a.whi + cbase;
         const int* wlo = a.wlo + cbase;
         const int t0 = w.t0, t1 = w.t1;
-        const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
-        const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
+        long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
+        long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
+        split_range(a.splits, w.s, La, Lb);
         const RecE64* recs = recs_all + cbase;
         int jj[P];
         double fj[P], acc[P];
@@ -1238,11 +1289,23 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_erf(StepArgs a) {
             }
             __syncwarp();
         }
-        double* out = a.out + size_t(w.c) * a.out_stride;
 #pragma unroll
         for (int p = 0; p < P; ++p)
-            if (jj[p] < t1) out[jj[p]] += acc[p];
+            if (jj[p] < t1) put_result(a, w.c, w.s, jj[p], acc[p]);
     }
+}
+
+// Sums the parts of split tiles in part order and adds them to out.
+__global__ void k_reduce_splits(StepArgs a, int ncond_out) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long pts = a.G.points;
+    if (i >= pts * ncond_out) return;
+    const int c = int(i / pts);
+    const long j = i - long(c) * pts;
+    const double* p = a.part + size_t(c) * a.splits * a.part_stride + size_t(j);
+    double v = 0.0;
+    for (int s = 0; s < a.splits; ++s) v += p[size_t(s) * a.part_stride];
+    a.out[size_t(c) * a.out_stride + size_t(a.G.start + j)] += v;
 }
 
 template <class K>
@@ -1367,6 +1430,13 @@ cudaError_t launch_grid_check(const GridDev& g, unsigned* err, cudaStream_t stre
     if (g.npoints_total < 2) return cudaSuccess;
     const int n = g.npoints_total - 1;
     k_grid_check<<<(n + 255) / 256, 256, 0, stream>>>(g, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_splits(const StepArgs& a, int ncond_out, cudaStream_t stream) {
+    if (a.splits <= 1 || a.G.points <= 0 || ncond_out <= 0) return cudaSuccess;
+    const long n = long(a.G.points) * ncond_out;
+    k_reduce_splits<<<unsigned((n + 255) / 256), 256, 0, stream>>>(a, ncond_out);
     return cudaGetLastError();
 }
 

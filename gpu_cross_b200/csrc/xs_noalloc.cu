@@ -177,6 +177,7 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
     sa.G = G;
     sa.tiles_per_cond = (grid->points + 32 * P - 1) / (32 * P);
     sa.n_items = sa.tiles_per_cond;
+    sa.splits = 1;  // the fixed array holds no split parts
     sa.counter = words + 1;
     sa.x0 = pa.x0;
     sa.xg = pa.xg;

@@ -566,6 +566,7 @@ int xs_server_create(int device, const xs_server_config* cfg, xs_server** out) {
     size_t scratch = xs_scratch_bytes_needed(&o, 1, c.chunk_lines);
     o.precision = XS_MIXED;
     scratch = std::max(scratch, xs_scratch_bytes_needed(&o, 1, c.chunk_lines));
+    scratch = ((scratch + 255) & ~size_t(255)) + (size_t(64) << 20);  // + the line-split parts
     for (int k = 0; k < c.lanes; ++k) {
         Lane ln;
         int rc = xs_engine_create(device, &ln.eng);

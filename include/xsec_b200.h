@@ -106,6 +106,12 @@ typedef struct {
     int conditions_per_warp; /* VOIGT batches: 0 = automatic, 1 = one condition
                                 per warp, 2/4/8 = that many conditions with the
                                 same cut evaluated together by each warp */
+    int line_splits;  /* 0 = automatic: when a call has too few grid tiles to
+                         fill the GPU (short or coarse grids over many lines),
+                         each tile's lines are split over up to 64 warps whose
+                         partial sums are added in a fixed order; 1 = never;
+                         N = N parts per tile.  The choice depends only on the
+                         call's sizes and the device's SM count. */
 } xs_options;
 
 /* Device-resident line list (structure of arrays, ascending nu). */

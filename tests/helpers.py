@@ -60,7 +60,7 @@ def to_device(lines, device):
 def run_engine(engine: capi.Engine, profile: int, lines, freq: np.ndarray, cond: dict, dfreq: float,
                device, convention=capi.CONV_GPU, precision=capi.FP64, cpu_threads=1,
                start_idx=0, points=None, intens0=None, half_width=0.1, P=0, W=0,
-               conds: list[dict] | None = None, C=0):
+               conds: list[dict] | None = None, C=0, S=0):
     """Run the engine once; returns the grid(s) as numpy."""
     import torch
 
@@ -74,7 +74,8 @@ def run_engine(engine: capi.Engine, profile: int, lines, freq: np.ndarray, cond:
     opts = capi.make_options(profile, dfreq, cond["mean_mass"], convention=convention,
                              precision=precision, cpu_threads=cpu_threads,
                              ref_temp=cond.get("ref_temp", 296.0), half_width=half_width,
-                             points_per_thread=P, warps_per_block=W, conditions_per_warp=C)
+                             points_per_thread=P, warps_per_block=W, conditions_per_warp=C,
+                             line_splits=S)
     cc = [capi.make_condition(c["temperature"], c["partition"], c.get("pressure", 1.0),
                               c.get("gamma_scale", 1.0), c.get("cut", -1.0)) for c in clist]
     grid = capi.make_grid(fr, start_idx, points)

@@ -49,6 +49,45 @@ def test_voigt_shapes_agree(engine, cuda, P):
         assert_fp64_parity(got, ref)
 
 
+@pytest.mark.parametrize("S", [1, 3, 64])
+def test_line_splits_vs_oracle(engine, cuda, S):
+    """A tile's lines split over S warps (partial sums added in split order)
+    give the oracle's result, and the same bits on every run."""
+    lines, grid, cond = small_voigt_case(seed=12, n=4000)
+    fr = grid.freq()
+    ref = oracle.gpu_convention(oracle.VOIGT, fr, np.zeros_like(fr), lines, cond, grid.dfreq)
+    got = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, S=S)
+    assert_fp64_parity(got, ref)
+    again = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, S=S)
+    assert np.array_equal(got, again)
+    mix = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, S=S,
+                     precision=capi.MIXED)
+    assert_mixed_parity(mix, ref)
+    dl = synth.exomol_like(2000, 3000, seed=13, nu_max=2000.0)
+    dg = synth.Grid(0.0, 2000.0, 20000)
+    dc = dict(temperature=296.0, partition=2844.0, mean_mass=30.01, pressure=1.0, ref_temp=296.0)
+    dref = oracle.gpu_convention(oracle.DOPPLER, dg.freq(), np.zeros(dg.npoints), dl, dc, dg.dfreq)
+    dgot = run_engine(engine, capi.DOPPLER, dl, dg.freq(), dc, dg.dfreq, cuda, S=S)
+    assert_fp64_parity(dgot, dref)
+
+
+def test_line_splits_multi_condition(engine, cuda):
+    lines = synth.random_lines(3000, 1000.0, 1100.0, 2500.0, 1e-6, 1e2, seed=52, pressure_atm=1.0)
+    grid = synth.Grid(990.0, 1110.0, 1200)
+    base = dict(mean_mass=17.03, pressure=1.0, ref_temp=296.0)
+    conds = [dict(base, temperature=t, partition=synth.partition_poly(t), gamma_scale=p, cut=25.0)
+             for t in (300.0, 2100.0) for p in (1e-3, 10.0)]
+    fr = grid.freq()
+    one = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, C=2, S=1,
+                     precision=capi.MIXED)
+    five = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, C=2, S=5,
+                      precision=capi.MIXED)
+    f64 = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, S=1)
+    for k in range(len(conds)):
+        assert_mixed_parity(one[k], f64[k])
+        assert_mixed_parity(five[k], f64[k])
+
+
 @pytest.mark.parametrize("threads", [1, 3, 8])
 def test_voigt_cpu_convention_vs_reference_openmp(engine, cuda, threads):
     lines, grid, cond = small_voigt_case(seed=3)

@@ -122,11 +122,12 @@ def test_same_result_alone_and_in_a_mix(cuda, molecule):
 
 def server_resident_bytes(lanes, chunk_lines):
     """What xs_server_create reserves: per lane the largest Voigt scratch
-    for chunk_lines lines plus 4 MiB."""
+    for chunk_lines lines, 64 MiB for line-split parts, plus 4 MiB."""
     need = 0
     for prec in (capi.FP64, capi.MIXED):
         o = capi.make_options(capi.VOIGT, 0.01, MASS, precision=prec)
         need = max(need, capi.lib().xs_scratch_bytes_needed(ctypes.byref(o), 1, chunk_lines))
+    need = (need + 255) // 256 * 256 + (64 << 20)
     return lanes * (need + (4 << 20))
 
 
