@@ -176,7 +176,7 @@ struct StepArgs {
     unsigned* counter;
     double x0, xg, x0g;  // Doppler / Gaussian constants
     // Line splits: with splits > 1 every tile is taken by `splits` work
-    // items, each over one contiguous part of the tile's lines; item s
+    // items, item s over the tile's 32-line groups s, s + splits, ...; it
     // stores its sums to part[(c * splits + s) * part_stride + j - G.start]
     // and k_reduce_splits adds the parts, in order, to out.
     int splits;

@@ -449,14 +449,12 @@ __device__ __forceinline__ bool next_item(const StepArgs& a, int P, int lane, Wo
     return true;
 }
 
-// The part [La, Lb) of a tile's lines that split s of `splits` takes.
-__device__ __forceinline__ void split_range(int splits, int s, long& La, long& Lb) {
-    if (splits <= 1) return;
-    const int nl = int(Lb - La);  // lines per tile < 2^31 (the engine limit)
-    const int per = (nl + splits - 1) / splits;
-    const int a0 = min(per * s, nl), b0 = min(per * (s + 1), nl);
-    Lb = La + b0;
-    La = La + a0;
+// Split s of `splits` takes the 32-line groups s, s + splits, s + 2 splits,
+// ... of the tile's lines [La, Lb): interleaved, so that the costly lines
+// near the tile (cores) are shared evenly between the splits.
+__device__ __forceinline__ int split_groups(long nl, int splits, int s) {
+    const int all = int((nl + 31) / 32);
+    return all > s ? (all - s + splits - 1) / splits : 0;
 }
 
 // Where item (c, s) puts the sum of grid point j: added to out, or stored to
@@ -669,15 +667,13 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
         const int* mi = a.mi;
         const int kc = a.kc[w.c];
         const int t0 = w.t0, t1 = w.t1, tl = t1 - 1;
-        long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
-        long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
+        const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
+        const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
         const long fs = warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; });
         const long Cb = warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; });
         const long fe = Cb > fs ? Cb : fs;
         const long E = warp_lower_bound(fs, fe, lane, [&](long i) { return mi[i] >= t0 - kc; });
         const long Fc = warp_lower_bound(E, fe, lane, [&](long i) { return mi[i] > tl + kc; });
-        // the runs above stay as found; the groups below clip them to the part
-        split_range(a.splits, w.s, La, Lb);
         const REC* recs = recs_all + cbase;
 
         int jj[P];
@@ -881,14 +877,15 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             }
         };
 
-        const long nl = Lb - La;
-        const int ngroups = int((nl + 31) / 32);
+        // this item's groups of 32 lines: gi-th starts at La + 32 (s + gi S)
+        const int ngroups = split_groups(Lb - La, a.splits, w.s);
+        auto gstart = [&](int gi) { return La + 32L * (w.s + long(gi) * a.splits); };
         // kStages-deep cp.async pipeline: groups gi+1 .. gi+kStages-1 are in
         // flight while group gi is evaluated (one commit per step, empty
         // commits past the end keep the group count uniform).
         auto issue = [&](int g) {
             if (g < ngroups) {
-                const long b = La + 32L * g;
+                const long b = gstart(g);
                 const long rem = Lb - b;
                 stage(buf + (g % kStages) * 32, recs + b, int(rem < 32 ? rem : 32), lane);
             }
@@ -901,7 +898,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             cp_async_wait<kStages - 1>();
             __syncwarp();
             const REC* R = buf + (gi % kStages) * 32;
-            const long gb = La + 32L * gi;
+            const long gb = gstart(gi);
             const long ge = Lb - gb < 32 ? Lb : gb + 32;
             auto lo_of = [&](long v) { return int((v < gb ? gb : (v > ge ? ge : v)) - gb); };
             const int a0 = lo_of(La), a1 = lo_of(fs);
@@ -1033,14 +1030,13 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
         int kc = 0;
 #pragma unroll
         for (int c = 0; c < C; ++c) kc = max(kc, a.kc[cg * C + c]);
-        long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
-        long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
+        const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
+        const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
         const long fs = warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; });
         const long Cb = warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; });
         const long fe = Cb > fs ? Cb : fs;
         const long E = warp_lower_bound(fs, fe, lane, [&](long i) { return mi[i] >= t0 - kc; });
         const long Fc = warp_lower_bound(E, fe, lane, [&](long i) { return mi[i] > tl + kc; });
-        split_range(a.splits, split, La, Lb);
         const LS* lsh = reinterpret_cast<const LS*>(a.lsh) + gbase;
         const CR* crec = reinterpret_cast<const CR*>(a.rec) + gbase * C;
 
@@ -1100,19 +1096,21 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
             push(deep, ax, T(r.y), T(r.pref), c);
         };
 
-        const long nl = Lb - La;
-        const int ngroups = int((nl + 31) / 32);
+        // this item's groups of 32 lines: gi-th starts at La + 32 (s + gi S)
+        const int ngroups = split_groups(Lb - La, a.splits, split);
+        auto gstart = [&](int gi) { return La + 32L * (split + long(gi) * a.splits); };
         auto stage_group = [&](int bufi, long b, int cnt) {
             stage(lsb + bufi * 32, lsh + b, cnt, lane);
             stage(crb + bufi * 32 * C, crec + b * C, cnt * C, lane);
         };
         if (ngroups > 0) {
-            stage_group(0, La, int(nl < 32 ? nl : 32));
+            const long b = gstart(0);
+            stage_group(0, b, int(Lb - b < 32 ? Lb - b : 32));
             cp_async_commit();
         }
         for (int gi = 0; gi < ngroups; ++gi) {
             if (gi + 1 < ngroups) {
-                const long b = La + 32L * (gi + 1);
+                const long b = gstart(gi + 1);
                 const long rem = Lb - b;
                 stage_group((gi + 1) & 1, b, int(rem < 32 ? rem : 32));
                 cp_async_commit();
@@ -1123,7 +1121,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
             __syncwarp();
             const LS* SL = lsb + (gi & 1) * 32;
             const CR* SC = crb + (gi & 1) * 32 * C;
-            const long gb = La + 32L * gi;
+            const long gb = gstart(gi);
             const long ge = Lb - gb < 32 ? Lb : gb + 32;
             auto lo_of = [&](long v) { return int((v < gb ? gb : (v > ge ? ge : v)) - gb); };
             const int a0 = lo_of(La), a1 = lo_of(fs), b1 = lo_of(E), c1 = lo_of(Fc), d1 = lo_of(fe),
@@ -1229,9 +1227,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_erf(StepArgs a) {
         const int* whi = a.whi + cbase;
         const int* wlo = a.wlo + cbase;
         const int t0 = w.t0, t1 = w.t1;
-        long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
-        long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
-        split_range(a.splits, w.s, La, Lb);
+        const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
+        const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
         const RecE64* recs = recs_all + cbase;
         int jj[P];
         double fj[P], acc[P];
@@ -1241,15 +1238,17 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_erf(StepArgs a) {
             fj[p] = F[jj[p] < t1 ? jj[p] : t1 - 1];
             acc[p] = 0.0;
         }
-        const long nl = Lb - La;
-        const int ngroups = int((nl + 31) / 32);
+        // this item's groups of 32 lines: gi-th starts at La + 32 (s + gi S)
+        const int ngroups = split_groups(Lb - La, a.splits, w.s);
+        auto gstart = [&](int gi) { return La + 32L * (w.s + long(gi) * a.splits); };
         if (ngroups > 0) {
-            stage(buf, recs + La, int(nl < 32 ? nl : 32), lane);
+            const long b = gstart(0);
+            stage(buf, recs + b, int(Lb - b < 32 ? Lb - b : 32), lane);
             cp_async_commit();
         }
         for (int gi = 0; gi < ngroups; ++gi) {
             if (gi + 1 < ngroups) {
-                const long b = La + 32L * (gi + 1);
+                const long b = gstart(gi + 1);
                 const long rem = Lb - b;
                 stage(buf + ((gi + 1) & 1) * 32, recs + b, int(rem < 32 ? rem : 32), lane);
                 cp_async_commit();
@@ -1259,7 +1258,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_erf(StepArgs a) {
             }
             __syncwarp();
             const RecE64* R = buf + (gi & 1) * 32;
-            const long gbase = La + 32L * gi;
+            const long gbase = gstart(gi);
             const int cnt = int(Lb - gbase < 32 ? Lb - gbase : 32);
             for (int t = 0; t < cnt; ++t) {
                 const double2* q = reinterpret_cast<const double2*>(&R[t]);
