@@ -574,7 +574,6 @@ struct WarpCoreQueue {
     using T = typename std::conditional<MIXED, float, double>::type;
     static constexpr int kCap = 32 * (P + 1);  // < 32 left + up to P rows of 32
     CoreEntry<T> q[kCap];
-    T val[32];
     T corr[P][32];
 };
 
@@ -586,8 +585,10 @@ template <int P, bool MIXED>
 __device__ __noinline__ int core_queue_flush(WarpCoreQueue<P, MIXED>& cq, int qn, int k, int lane) {
     using T = typename WarpCoreQueue<P, MIXED>::T;
     T v = T(0);
+    int dest = 0;
     if (lane < k) {
         const CoreEntry<T> e = cq.q[lane];
+        dest = e.dest;
         if (MIXED) {
             // only regions III and IV are queued on the mixed path
             const float ax = float(e.x), y = float(e.y);
@@ -598,11 +599,21 @@ __device__ __noinline__ int core_queue_flush(WarpCoreQueue<P, MIXED>& cq, int qn
             v = T(w4_re(double(e.x), double(e.y)) * double(e.pref));
         }
     }
-    cq.val[lane] = v;
-    __syncwarp();
-    for (int i = 0; i < k; ++i) {
-        const int d = cq.q[i].dest;
-        if ((d & 31) == lane) cq.corr[d >> 5][lane] += cq.val[i];
+    // Each push queued a run of consecutive lanes of one row, so the queue is
+    // a sequence of runs (entry s + i is lane first + i).  Runs are visited in
+    // queue order and each lane takes at most one entry per run: every lane's
+    // correction column gets its entries in queue order.
+    const int prev = __shfl_up_sync(0xffffffffu, dest, 1);
+    const bool start = lane < k && (lane == 0 || dest != prev + 1 || (dest & 31) == 0);
+    unsigned starts = __ballot_sync(0xffffffffu, start);
+    while (starts) {
+        const int s0 = __ffs(starts) - 1;
+        starts &= starts - 1;
+        const int e0 = starts ? __ffs(starts) - 1 : k;
+        const int d0 = __shfl_sync(0xffffffffu, dest, s0);
+        const int first = d0 & 31, row = d0 >> 5;
+        const T vv = __shfl_sync(0xffffffffu, v, (s0 + lane - first) & 31);
+        if (lane >= first && lane < first + (e0 - s0)) cq.corr[row][lane] += vv;
     }
     __syncwarp();
     const int rem = qn - k;

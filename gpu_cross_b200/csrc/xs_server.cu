@@ -124,32 +124,39 @@ double overlap_sum(const LineIndex& L, const size_t idx[4], const double p[4], d
 struct ChunkPlan {
     int start, points;
     size_t l0, l1;  // line slice
-    double pairs;   // estimated line-evals
+    double pairs;   // estimated line-evals inside the window (what is reported)
+    double cost;    // estimated work: line-evals inside the cost window
 };
 
-// Greedy over tiles: a chunk takes tiles while its estimated line-evals stay
+// Greedy over tiles: a chunk takes tiles while its estimated work stays
 // within max_pairs and its line slice within max_lines (at least one tile).
+// The work is counted over [nu - cost_cut, nu + cost_cut]: the window for
+// Voigt, the span where Doppler pairs are not skipped as exact zeros.
 void plan_chunks(const LineIndex& L, double f0, double df, int npoints, double cut,
-                 double max_pairs, size_t max_lines, std::vector<ChunkPlan>& out) {
+                 double cost_cut, double max_pairs, size_t max_lines, std::vector<ChunkPlan>& out) {
     out.clear();
     const double margin = 2.0 * df;
     auto freq = [&](long i) { return f0 + double(i) * df; };
-    Cursor bp[4], c_lo, c_hi;
+    Cursor bp[4], bq[4], c_lo, c_hi;
     const int ntiles = (npoints + kTile - 1) / kTile;
-    ChunkPlan cur{0, 0, 0, 0, 0.0};
+    ChunkPlan cur{0, 0, 0, 0, 0.0, 0.0};
+    auto tile_sum = [&](Cursor* cs, double a, double b, double h) {
+        // breakpoints in ascending order; a + h and b - h swap when the tile
+        // is wider than the window
+        double p[4] = {a - h, std::min(a + h, b - h), std::max(a + h, b - h), b + h};
+        size_t idx[4];
+        for (int k = 0; k < 4; ++k) idx[k] = cs[k].seek(L, p[k], false);
+        return overlap_sum(L, idx, p, a, b, h) / df;
+    };
     for (int t = 0; t < ntiles; ++t) {
         const int s = t * kTile, e = std::min(npoints, s + kTile);
         const double a = freq(s) - 0.5 * df, b = freq(e - 1) + 0.5 * df;
-        // breakpoints in ascending order; a + cut and b - cut swap when the
-        // tile is wider than the window
-        double p[4] = {a - cut, std::min(a + cut, b - cut), std::max(a + cut, b - cut), b + cut};
-        size_t idx[4];
-        for (int k = 0; k < 4; ++k) idx[k] = bp[k].seek(L, p[k], false);
-        const double tp = overlap_sum(L, idx, p, a, b, cut) / df;
+        const double tp = tile_sum(bp, a, b, cut);
+        const double tc = cost_cut < cut ? tile_sum(bq, a, b, cost_cut) : tp;
         const size_t l1 = c_hi.seek(L, freq(e - 1) + cut + margin, true);
-        if (cur.points > 0 && (cur.pairs + tp > max_pairs || l1 - cur.l0 > max_lines)) {
+        if (cur.points > 0 && (cur.cost + tc > max_pairs || l1 - cur.l0 > max_lines)) {
             out.push_back(cur);
-            cur = ChunkPlan{s, 0, 0, 0, 0.0};
+            cur = ChunkPlan{s, 0, 0, 0, 0.0, 0.0};
         }
         if (cur.points == 0) {
             cur.start = s;
@@ -158,6 +165,7 @@ void plan_chunks(const LineIndex& L, double f0, double df, int npoints, double c
         cur.points = e - cur.start;
         cur.l1 = l1;
         cur.pairs += tp;
+        cur.cost += tc;
     }
     out.push_back(cur);
 }
@@ -451,8 +459,8 @@ bool issue(xs_server* s, Request* r) {
             r->next = r->chunks.size();  // nothing more to run
         }
     }
-    r->remaining -= c.pairs;
-    ln.load -= c.pairs;
+    r->remaining -= c.cost;
+    ln.load -= c.cost;
     const bool last = r->next >= r->chunks.size();
     if (last && r->status == XS_OK) {
         if (cudaMemcpyAsync(s->arena.at(r->host_off), r->d_out, sizeof(double) * size_t(r->q.npoints),
@@ -743,7 +751,18 @@ int xs_server_submit(xs_server* s, const xs_request* q, unsigned long long* requ
     r->cond.cut = q->cut;
     const double cut = q->cut > 0.0 ? q->cut
                                      : (q->profile == XS_VOIGT ? std::fmin(25.0 * q->pressure, 100.0) : 100.0);
-    plan_chunks(m.index(), q->f0, q->df, q->npoints, cut, s->cfg.chunk_pairs, s->cfg.chunk_lines, r->chunks);
+    // Doppler pairs beyond ~6 Doppler widths add exactly 0 and are skipped
+    // (the erf saturation of step one), so their work is counted over that
+    // span: nu_max * 6 sqrt(2 k T N_A / M) / c plus the bin and a margin.
+    double cost_cut = cut;
+    if (q->profile == XS_DOPPLER) {
+        const double kB = 1.380658e-16, NA = 6.0221412927e23, c = 2.99792458e10;
+        const double nu_max = q->f0 + double(q->npoints) * q->df + cut;
+        const double w = 6.0 * std::sqrt(2.0 * kB * q->temperature * NA / m.mass) / c;
+        cost_cut = std::fmin(cut, std::fabs(nu_max) * w * 1.01 + 2.5 * q->df);
+    }
+    plan_chunks(m.index(), q->f0, q->df, q->npoints, cut, cost_cut, s->cfg.chunk_pairs,
+                s->cfg.chunk_lines, r->chunks);
     for (const ChunkPlan& c : r->chunks) {
         if (c.l1 - c.l0 > s->cfg.chunk_lines) {
             delete r;
@@ -751,8 +770,8 @@ int xs_server_submit(xs_server* s, const xs_request* q, unsigned long long* requ
                                        "than chunk_lines");
         }
         r->pairs += c.pairs;
+        r->remaining += c.cost;
     }
-    r->remaining = r->pairs;
     r->lines = m.index().upper(q->f0 + double(q->npoints - 1) * q->df + cut) -
                m.index().lower(q->f0 - cut);
     r->dev_bytes = request_device_bytes(*q);
@@ -830,7 +849,7 @@ int xs_plan_chunks(const double* nu, size_t n, double f0, double df, int npoints
     L.cum = cum.data();
     L.n = n;
     std::vector<ChunkPlan> plan;
-    plan_chunks(L, f0, df, npoints, cut, max_pairs, max_lines ? max_lines : SIZE_MAX, plan);
+    plan_chunks(L, f0, df, npoints, cut, cut, max_pairs, max_lines ? max_lines : SIZE_MAX, plan);
     *nchunks = int(plan.size());
     if (int(plan.size()) > cap) return sfail(XS_ERR_INVALID, "xs_plan_chunks: more chunks than cap");
     for (size_t k = 0; k < plan.size(); ++k) {

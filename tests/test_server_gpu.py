@@ -42,8 +42,9 @@ def subset(lines, lo, hi):
                                         (capi.DOPPLER, capi.FP64)])
 def test_server_matches_oracle(cuda, molecule, prof, prec):
     T, Q, P, f0, df, n, cut = 900.0, 1234.5, 2.0, 1000.0, 0.01, 12000, 25.0
-    # small chunks: the request runs as many chunks
-    srv = capi.Server(0, lanes=2, chunk_pairs=2e6)
+    # small chunks: the request runs as many chunks (Doppler work is counted
+    # over the few Doppler widths where pairs are not exactly zero)
+    srv = capi.Server(0, lanes=2, chunk_pairs=2e6 if prof == capi.VOIGT else 2e3)
     try:
         mid = srv.add_molecule(molecule, MASS)
         rid = srv.submit(mid, prof, prec, T, Q, P, f0, df, n, cut=cut)
