@@ -1046,8 +1046,10 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
         const long fs = warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; });
         const long Cb = warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; });
         const long fe = Cb > fs ? Cb : fs;
-        const long E = warp_lower_bound(fs, fe, lane, [&](long i) { return mi[i] >= t0 - kc; });
-        const long Fc = warp_lower_bound(E, fe, lane, [&](long i) { return mi[i] > tl + kc; });
+        // core candidates among all the tile's lines (partial ones included):
+        // only lines in [E, Fc) can have a core band that reaches the row
+        const long E = warp_lower_bound(La, Lb, lane, [&](long i) { return mi[i] >= t0 - kc; });
+        const long Fc = warp_lower_bound(E, Lb, lane, [&](long i) { return mi[i] > tl + kc; });
         const LS* lsh = reinterpret_cast<const LS*>(a.lsh) + gbase;
         const CR* crec = reinterpret_cast<const CR*>(a.rec) + gbase * C;
 
@@ -1137,55 +1139,65 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
             auto lo_of = [&](long v) { return int((v < gb ? gb : (v > ge ? ge : v)) - gb); };
             const int a0 = lo_of(La), a1 = lo_of(fs), b1 = lo_of(E), c1 = lo_of(Fc), d1 = lo_of(fe),
                       e1 = lo_of(Lb);
-            // fast lines: window covers the row, no core near it
-            {
-                int t = a1;
-                for (; t < b1; ++t) {
+            // Runs of this group: [a1, d1) cover the row (full), the rest
+            // are partial; [b1, c1) are the core candidates.
+            // Full lines away from every core: region I with no test.
+            auto fast_run = [&](int x, int y) {
+                for (int t = x; t < y; ++t) {
                     const LS s = SL[t];
 #pragma unroll
                     for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], T(1), c);
                 }
-                for (t = c1; t < d1; ++t) {
+            };
+            // Partial lines away from every core: region I, the window as a
+            // lane mask.
+            auto masked_run = [&](int x, int y) {
+                for (int t = x; t < y; ++t) {
                     const LS s = SL[t];
+                    const T mask = (jj >= s.lo && jj < s.hi && jj < t1) ? T(1) : T(0);
 #pragma unroll
-                    for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], T(1), c);
+                    for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], mask, c);
                 }
-            }
-            // core-candidate lines (window covers the row) and partial lines.
-            // Per condition: when its core band misses the row (the usual
-            // case for partial lines, whose centres lie about a cut away),
-            // region I with the window as a lane mask; otherwise the
+            };
+            // Core candidates.  Per condition: when its core band misses the
+            // row, region I with the window as a lane mask; otherwise the
             // lane-by-lane core path.
-            for (int t = a0; t < e1; ++t) {
-                if (t == a1) t = b1;
-                if (t == c1) t = d1;
-                if (t >= e1) break;
-                const LS s = SL[t];
-                const bool full = (t >= b1 && t < c1);
-                const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
-                const T mask = in ? T(1) : T(0);
-                int mline;
-                if constexpr (MIXED) mline = int(s.m);  // exact below 2^24; "whole" lines have unbounded bands
-                else mline = mi[gb + t];
-                bool any_core = false;
+            auto cand_run = [&](int x, int y) {
+                for (int t = x; t < y; ++t) {
+                    const LS s = SL[t];
+                    const bool full = (t >= a1 && t < d1);
+                    const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
+                    const T mask = in ? T(1) : T(0);
+                    int mline;
+                    if constexpr (MIXED) mline = int(s.m);  // exact below 2^24; "whole" lines have unbounded bands
+                    else mline = mi[gb + t];
+                    bool any_core = false;
 #pragma unroll
-                for (int c = 0; c < C; ++c) {
-                    const CR& r = SC[t * C + c];
-                    bool hit = false;
-                    if (r.core != -1) {
-                        const int aa = r.core & 0xffff, bb = (r.core >> 16) & 0xffff;
-                        hit = (aa == 0x7fff || mline - aa <= tl) && (bb == 0x7fff || mline + bb >= t0);
+                    for (int c = 0; c < C; ++c) {
+                        const CR& r = SC[t * C + c];
+                        bool hit = false;
+                        if (r.core != -1) {
+                            const int aa = r.core & 0xffff, bb = (r.core >> 16) & 0xffff;
+                            hit = (aa == 0x7fff || mline - aa <= tl) && (bb == 0x7fff || mline + bb >= t0);
+                        }
+                        if (!hit) {
+                            region1(offset(s, r), r, mask, c);
+                        } else {
+                            core_cond(s, r, mline, in, c);
+                            any_core = true;
+                        }
                     }
-                    if (!hit) {
-                        region1(offset(s, r), r, mask, c);
-                    } else {
-                        core_cond(s, r, mline, in, c);
-                        any_core = true;
-                    }
+                    if (any_core)
+                        while (qn >= 32) qn = core_queue_flush<C, MIXED>(cq, qn, 32, lane);
                 }
-                if (any_core)
-                    while (qn >= 32) qn = core_queue_flush<C, MIXED>(cq, qn, 32, lane);
-            }
+            };
+            fast_run(a1, min(d1, b1));
+            fast_run(max(a1, c1), d1);
+            masked_run(a0, min(a1, b1));
+            masked_run(max(a0, c1), a1);
+            masked_run(d1, min(e1, b1));
+            masked_run(max(d1, c1), e1);
+            cand_run(b1, c1);
             if (MIXED) {
                 if (qn > 0) qn = core_queue_flush<C, MIXED>(cq, qn, qn, lane);
 #pragma unroll
