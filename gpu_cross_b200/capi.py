@@ -78,6 +78,11 @@ class RequestInfo(ctypes.Structure):
                 ("line_evals", ctypes.c_double), ("lines", ctypes.c_size_t)]
 
 
+class StreamStats(ctypes.Structure):
+    _fields_ = [("total_ms", ctypes.c_double), ("copy_span_ms", ctypes.c_double),
+                ("h2d_bytes", ctypes.c_double), ("chunks", ctypes.c_int)]
+
+
 _VP = ctypes.c_void_p
 _I = ctypes.c_int
 _D = ctypes.c_double
@@ -111,6 +116,9 @@ _SIGS = {
     "xs_measure_peaks": (_I, [_I, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "xs_execute_noalloc": (_I, [ctypes.POINTER(Options), ctypes.POINTER(Condition),
                                 ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _VP]),
+    "xs_stream_execute": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _VP, _VP,
+                               _VP, _SZ, ctypes.POINTER(GridC), _VP, _SZ,
+                               ctypes.POINTER(StreamStats)]),
     "xs_manager_create": (_I, [_I, _I, _I, _I, _SZ, ctypes.POINTER(_VP)]),
     "xs_manager_destroy": (_I, [_VP]),
     "xs_manager_set_precision": (_I, [_VP, _I]),
@@ -216,6 +224,16 @@ class Engine:
         arr = (Condition * len(conds))(*conds)
         check(lib().xs_engine_execute(self.h, ctypes.byref(opts), arr, len(conds),
                                       ctypes.byref(lines), ctypes.byref(grid), out_ptr, out_stride))
+
+    def stream_execute(self, opts: Options, cond: Condition, h_nu: int, h_s: int, h_gamma: int,
+                       n: int, grid: GridC, out_ptr: int, chunk_lines: int) -> dict:
+        """xs_stream_execute over host arrays given by address (f64 centres,
+        f32 intensities, f32 Lorentz widths; pinned for overlapped copies)."""
+        st = StreamStats()
+        check(lib().xs_stream_execute(self.h, ctypes.byref(opts), ctypes.byref(cond), h_nu, h_s,
+                                      h_gamma, n, ctypes.byref(grid), out_ptr, chunk_lines,
+                                      ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in StreamStats._fields_}
 
     def capture(self, opts: Options, conds: list[Condition], lines: Lines, grid: GridC, out_ptr: int,
                 out_stride: int = 0, zero_out: bool = True) -> "Graph":

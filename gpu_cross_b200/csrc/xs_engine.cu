@@ -299,9 +299,12 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         return fail(XS_ERR_INVALID, "grid chunk outside the grid");
     if (ncond > 1 && out_stride < size_t(grid->npoints_total))
         return fail(XS_ERR_INVALID, "out_stride smaller than the grid");
-    if (lines->count > 0 && (!lines->nu || !lines->energies || !lines->aif || !lines->gns))
+    const bool streamed = ov && ov->s32;
+    if (streamed && (kind != XS_VOIGT || opt->convention != XS_CONV_GPU || !ov->gl32))
+        return fail(XS_ERR_UNSUPPORTED, "precomputed intensities: VOIGT, GPU convention, with gamma");
+    if (lines->count > 0 && (!lines->nu || (!streamed && (!lines->energies || !lines->aif || !lines->gns))))
         return fail(XS_ERR_INVALID, "line arrays missing");
-    if (kind == XS_VOIGT && lines->count > 0 && (!lines->gamma || !lines->n))
+    if (kind == XS_VOIGT && lines->count > 0 && !streamed && (!lines->gamma || !lines->n))
         return fail(XS_ERR_INVALID, "VOIGT needs gamma and n");
     if (lines->count > size_t(INT32_MAX))
         return fail(XS_ERR_INVALID, "more than 2^31-1 lines in one call");
@@ -439,6 +442,8 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     L.nexp = lines->n;
     L.gns = lines->gns;
     L.n = n;
+    L.s32 = streamed ? ov->s32 : nullptr;
+    L.gl32 = streamed ? ov->gl32 : nullptr;
 
     const cudaStream_t st = e->stream;
     const bool timing = !(ov && ov->no_timing);
@@ -553,6 +558,7 @@ int engine_reserve(xs_engine* e, size_t bytes) {
 }
 
 int engine_device(const xs_engine* e) { return e ? e->device : -1; }
+void* engine_stream(const xs_engine* e) { return e ? static_cast<void*>(e->stream) : nullptr; }
 
 }  // namespace xs
 

@@ -20,6 +20,8 @@ struct ExecOverride {
     bool use_consts = false;      // take cmcoef and beta from below instead of
     double cmcoef = 0.0;          //   recomputing them from T (launcher level:
     double beta = 0.0;            //   the cross_section_data the caller copied)
+    const float* s32 = nullptr;   // streamed Voigt lines: S(T) and gamma(T, P)
+    const float* gl32 = nullptr;  //   per line (see LinesDev)
 };
 
 int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
@@ -31,6 +33,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
 int engine_reserve(xs_engine* e, size_t bytes);
 // The engine's device and stream.
 int engine_device(const xs_engine* e);
+void* engine_stream(const xs_engine* e);
 
 int set_error(int code, const char* msg);
 CondDev make_cond(const xs_options& o, const xs_condition& c);

@@ -137,6 +137,11 @@ struct LinesDev {
     const double *nu, *energies, *aif, *gamma, *nexp;
     const int* gns;
     long n;  // lines evaluated (may be less than uploaded: CPU coverage rule)
+    // Streamed lists (Voigt, GPU convention): the intensity S(T) and the
+    // Lorentz half width gamma(T, P) of the condition, precomputed in FP32;
+    // when set, energies, aif, gns, gamma and nexp are not read.
+    const float* s32;
+    const float* gl32;
 };
 
 struct PrepArgs {

@@ -136,9 +136,10 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c) {
     const int s = a.G.start, e = a.G.start + a.G.points;
     const double nu = a.L.nu[i];
     if (c == 0 && i > 0 && nu < a.L.nu[i - 1]) atomicOr(a.err, kErrUnsorted);
-    const double ei = a.L.energies[i];
-    const double aif = a.L.aif[i];
-    const double gns = double(a.L.gns[i]);
+    const bool streamed = KIND == kVoigt && CONV == kConvGpu && a.L.s32 != nullptr;
+    const double ei = streamed ? 0.0 : a.L.energies[i];
+    const double aif = streamed ? 0.0 : a.L.aif[i];
+    const double gns = streamed ? 0.0 : double(a.L.gns[i]);
     const double cut = C.cut;
     const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
     int kcl = 0;
@@ -151,9 +152,13 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c) {
             // device_compute_cross_section_voigt_stepone, cross_kernal.cu:775-779
             double nu_if = nu;
             if (nu_if == 0) nu_if = 1e-6;
-            S = C.cmcoef * aif * gns * kISQRTPI * exp(-C.beta * ei) * (1.0 - exp(-C.beta * nu_if)) /
-                (nu_if * nu_if * C.partition);
-            if (gns == -1) S = aif;
+            if (streamed) {
+                S = double(a.L.s32[i]);
+            } else {
+                S = C.cmcoef * aif * gns * kISQRTPI * exp(-C.beta * ei) * (1.0 - exp(-C.beta * nu_if)) /
+                    (nu_if * nu_if * C.partition);
+                if (gns == -1) S = aif;
+            }
         } else {
             // doppler_stepone / stepone, cross_kernal.cu:645-648, :487-490
             S = C.cmcoef * aif * gns * exp(-C.beta * ei) * (1.0 - exp(-C.beta * nu)) /
@@ -196,7 +201,8 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c) {
     }
 
     if (KIND == kVoigt) {
-        const double gl = a.L.gamma[i] * C.gamma_scale * pow(C.tratio, a.L.nexp[i]);
+        const double gl = streamed ? double(a.L.gl32[i])
+                                   : a.L.gamma[i] * C.gamma_scale * pow(C.tratio, a.L.nexp[i]);
         const double g = 1.0 / (nu_p * C.dpw);  // gammaG, cross_kernal.cu:958
         const double y = gl * g;
         const double pref = (CONV == kConvCpu && S == 0.0) ? 0.0 : S * g;

@@ -235,6 +235,28 @@ int xs_measure_peaks(int device, double* fp32_tflops, double* fp64_tflops, doubl
 int xs_execute_noalloc(const xs_options* opt, const xs_condition* cond, const xs_lines* lines,
                        const xs_grid* grid, double* out, void* stream);
 
+/* Streamed Voigt line list (no counterpart in the reference, which hands the
+ * manager one host chunk at a time and waits, VoigtProfile.cpp:56-103): the
+ * lines stay in host memory -- pinned, for copies that overlap compute -- as
+ * FP64 centres (ascending), FP32 intensities S(T) and FP32 Lorentz half widths
+ * gamma(T, P) of the one condition `cond` (T, Q and P there only set the
+ * Doppler width and the cut).  They are copied chunk_lines at a time into two
+ * device buffers on a second stream while the previous chunk is evaluated on
+ * the engine's stream; every chunk adds into `out` (the whole grid, device)
+ * the points its lines reach.  VOIGT, GPU convention, FP64 or mixed.  Blocks
+ * until done; `stats` (may be NULL) gets the device time of the whole
+ * pipeline, the copy stream's span and the bytes copied. */
+typedef struct {
+    double total_ms;      /* first copy issued -> last chunk evaluated */
+    double copy_span_ms;  /* first copy issued -> last copy done */
+    double h2d_bytes;
+    int chunks;
+} xs_stream_stats;
+int xs_stream_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond,
+                      const double* h_nu, const float* h_s, const float* h_gamma, size_t n,
+                      const xs_grid* grid, double* out, size_t chunk_lines,
+                      xs_stream_stats* stats);
+
 /* ---- 3. manager level: BaseManager over host buffers --------------------- */
 /* kind: 0 = GpuManager (reference GPU convention), 1 = OpenMPManager
  * (reference CPU convention, computed on the GPU). */
