@@ -134,6 +134,8 @@ _SIGS = {
     "xs_server_create": (_I, [_I, ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
     "xs_server_destroy": (_I, [_VP]),
     "xs_server_add_molecule": (_I, [_VP] + [_VP] * 6 + [_SZ, _D, _D, ctypes.POINTER(_I)]),
+    "xs_server_add_states": (_I, [_VP, _I, _VP, _VP, _SZ]),
+    "xs_partition_sum": (_I, [_I, _VP, _VP, _SZ, _VP, _I, _VP]),
     "xs_server_submit": (_I, [_VP, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_ulonglong)]),
     "xs_server_wait": (_I, [_VP, ctypes.c_ulonglong, _VP, _I, ctypes.POINTER(RequestInfo), _I]),
     "xs_server_pending": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
@@ -424,6 +426,13 @@ class Server:
                                            mean_mass, ref_temp, ctypes.byref(mid)))
         return mid.value
 
+    def add_states(self, molecule: int, energies, gns) -> None:
+        import numpy as np
+
+        e = np.ascontiguousarray(energies, np.float64)
+        g = np.ascontiguousarray(gns, np.int32)
+        check(lib().xs_server_add_states(self.h, molecule, e.ctypes.data, g.ctypes.data, e.size))
+
     def submit(self, molecule: int, profile: int, precision: int, temperature: float,
                partition: float, pressure: float, f0: float, df: float, npoints: int,
                cut: float = -1.0) -> int:
@@ -447,3 +456,17 @@ class Server:
         q, a = ctypes.c_int(), ctypes.c_int()
         check(lib().xs_server_pending(self.h, ctypes.byref(q), ctypes.byref(a)))
         return q.value, a.value
+
+
+def partition_sum(energies, gns, temperatures, device: int = 0):
+    """xs_partition_sum: Q(T) for each temperature from a state list."""
+    import numpy as np
+
+    e = np.ascontiguousarray(energies, np.float64)
+    g = np.ascontiguousarray(gns, np.int32)
+    t = np.ascontiguousarray(np.atleast_1d(temperatures), np.float64)
+    q = np.empty(t.size)
+    check(lib().xs_partition_sum(device, e.ctypes.data if e.size else None,
+                                 g.ctypes.data if g.size else None, e.size, t.ctypes.data, t.size,
+                                 q.ctypes.data))
+    return q

@@ -36,6 +36,13 @@
 #include "xs_engine.h"
 #include "xsec_b200.h"
 
+namespace xs {
+cudaError_t partition_on_stream(const double* d_e, const int* d_g, long n, const double* d_beta,
+                                int n_temps, double* d_q, double* work, cudaStream_t stream);
+size_t partition_work_doubles(int n_temps);
+double partition_beta(double temperature);
+}  // namespace xs
+
 namespace {
 
 using Clock = std::chrono::steady_clock;
@@ -236,6 +243,11 @@ struct Molecule {
     double mass = 0.0, ref_temp = 296.0;
     std::vector<double> h_nu, h_cum;
     size_t bytes = 0;
+    // optional state list (xs_server_add_states) for Q(T), cached per T
+    double* d_se = nullptr;
+    int* d_sg = nullptr;
+    size_t ns = 0;
+    std::map<double, double> qcache;
     LineIndex index() const {
         LineIndex L;
         L.nu = h_nu.data();
@@ -301,6 +313,11 @@ struct xs_server {
     std::thread worker;
     std::atomic<bool> stop{false};
     std::atomic<int> n_queued{0}, n_active{0};
+
+    // partition functions of molecules with states: one at a time
+    std::mutex qmu;
+    cudaStream_t aux = nullptr;
+    double* d_pwork = nullptr;  // beta, Q and the block sums of one temperature
 };
 
 namespace {
@@ -547,6 +564,38 @@ void scheduler(xs_server* s) {
     }
 }
 
+// Q(T) of a molecule from its states, computed on the device once per T.
+int molecule_partition(xs_server* s, int mol, double temperature, double* q) {
+    std::lock_guard<std::mutex> lk(s->qmu);
+    Molecule& m = s->mols[size_t(mol)];
+    if (!m.d_se)
+        return sfail(XS_ERR_INVALID, "xs_server_submit: partition <= 0 needs the molecule's states "
+                                     "(xs_server_add_states)");
+    auto it = m.qcache.find(temperature);
+    if (it != m.qcache.end()) {
+        *q = it->second;
+        return XS_OK;
+    }
+    DevGuard dg(s->device);
+    const double beta = xs::partition_beta(temperature);
+    double* d_beta = s->d_pwork;
+    double* d_q = s->d_pwork + 1;
+    double* work = s->d_pwork + 2;
+    cudaError_t err = cudaMemcpyAsync(d_beta, &beta, sizeof(double), cudaMemcpyHostToDevice, s->aux);
+    if (err == cudaSuccess) err = xs::partition_on_stream(m.d_se, m.d_sg, long(m.ns), d_beta, 1, d_q, work, s->aux);
+    double val = 0.0;
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&val, d_q, sizeof(double), cudaMemcpyDeviceToHost, s->aux);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s->aux);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return sfail(XS_ERR_CUDA, std::string("partition function: ") + cudaGetErrorString(err));
+    }
+    if (m.qcache.size() > 4096) m.qcache.clear();
+    m.qcache[temperature] = val;
+    *q = val;
+    return XS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -624,6 +673,18 @@ int xs_server_create(int device, const xs_server_config* cfg, xs_server** out) {
         delete s;
         return sfail(XS_ERR_NOMEM, "xs_server_create: pinned host arena");
     }
+    if (cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&s->d_pwork, (2 + xs::partition_work_doubles(1)) * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        if (s->aux) cudaStreamDestroy(s->aux);
+        for (Lane& l : s->lanes) {
+            xs_engine_destroy(l.eng);
+            cudaStreamDestroy(l.st);
+        }
+        s->arena.release();
+        delete s;
+        return sfail(XS_ERR_NOMEM, "xs_server_create: partition work area");
+    }
     s->worker = std::thread(scheduler, s);
     *out = s;
     return XS_OK;
@@ -645,7 +706,11 @@ int xs_server_destroy(xs_server* s) {
         cudaStreamDestroy(l.st);
     }
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    if (s->aux) cudaStreamDestroy(s->aux);
+    cudaFree(s->d_pwork);
     for (Molecule& m : s->mols) {
+        cudaFree(m.d_se);
+        cudaFree(m.d_sg);
         cudaFree(m.nu);
         cudaFree(m.e);
         cudaFree(m.a);
@@ -715,6 +780,41 @@ int xs_server_add_molecule(xs_server* s, const double* nu, const double* energie
     return XS_OK;
 }
 
+int xs_server_add_states(xs_server* s, int molecule_id, const double* energies, const int* gns,
+                         size_t count) {
+    if (!s || !energies || !gns || count == 0)
+        return sfail(XS_ERR_INVALID, "xs_server_add_states: NULL argument or no states");
+    DevGuard dg(s->device);
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::lock_guard<std::mutex> lq(s->qmu);
+    if (molecule_id < 0 || size_t(molecule_id) >= s->mols.size())
+        return sfail(XS_ERR_INVALID, "xs_server_add_states: no such molecule");
+    Molecule& m = s->mols[size_t(molecule_id)];
+    const size_t bytes = count * (sizeof(double) + sizeof(int));
+    if (s->resident + s->dev_requests + bytes > s->cfg.device_budget)
+        return sfail(XS_ERR_NOMEM, "xs_server_add_states: over the device budget");
+    double* de = nullptr;
+    int* dg2 = nullptr;
+    cudaError_t err = cudaMalloc(&de, count * sizeof(double));
+    if (err == cudaSuccess) err = cudaMalloc(&dg2, count * sizeof(int));
+    if (err == cudaSuccess) err = cudaMemcpy(de, energies, count * sizeof(double), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(dg2, gns, count * sizeof(int), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(de);
+        cudaFree(dg2);
+        return sfail(XS_ERR_CUDA, std::string("xs_server_add_states: ") + cudaGetErrorString(err));
+    }
+    cudaFree(m.d_se);
+    cudaFree(m.d_sg);
+    m.d_se = de;
+    m.d_sg = dg2;
+    m.ns = count;
+    m.qcache.clear();
+    s->resident += bytes;
+    return XS_OK;
+}
+
 int xs_server_submit(xs_server* s, const xs_request* q, unsigned long long* request_id) {
     if (!s || !q || !request_id) return sfail(XS_ERR_INVALID, "xs_server_submit: NULL argument");
     const auto t0 = Clock::now();
@@ -730,11 +830,16 @@ int xs_server_submit(xs_server* s, const xs_request* q, unsigned long long* requ
         return sfail(XS_ERR_UNSUPPORTED, "xs_server_submit: profile must be VOIGT or DOPPLER");
     if (q->precision != XS_FP64 && q->precision != XS_MIXED)
         return sfail(XS_ERR_INVALID, "xs_server_submit: precision");
-    if (!(q->temperature > 0.0) || !(q->partition > 0.0) || !(q->df > 0.0) || q->npoints < 1 ||
-        !(q->pressure > 0.0))
-        return sfail(XS_ERR_INVALID, "xs_server_submit: T, Q, P and df must be > 0, npoints >= 1");
+    if (!(q->temperature > 0.0) || !(q->df > 0.0) || q->npoints < 1 || !(q->pressure > 0.0))
+        return sfail(XS_ERR_INVALID, "xs_server_submit: T, P and df must be > 0, npoints >= 1");
+    double partition = q->partition;
+    if (!(partition > 0.0)) {
+        const int rc = molecule_partition(s, q->molecule, q->temperature, &partition);
+        if (rc != XS_OK) return rc;
+    }
     auto* r = new Request();
     r->q = *q;
+    r->q.partition = partition;
     const Molecule& m = s->mols[size_t(q->molecule)];
     r->opt.profile = q->profile;
     r->opt.convention = XS_CONV_GPU;
@@ -745,7 +850,7 @@ int xs_server_submit(xs_server* s, const xs_request* q, unsigned long long* requ
     r->opt.half_width = 0.1;
     r->opt.dfreq = q->df;
     r->cond.temperature = q->temperature;
-    r->cond.partition = q->partition;
+    r->cond.partition = partition;
     r->cond.pressure = q->pressure;
     r->cond.gamma_scale = q->pressure;
     r->cond.cut = q->cut;

@@ -257,6 +257,13 @@ int xs_stream_execute(xs_engine* e, const xs_options* opt, const xs_condition* c
                       const xs_grid* grid, double* out, size_t chunk_lines,
                       xs_stream_stats* stats);
 
+/* Partition functions on the device: q[t] = sum_i gns[i] exp(-c2 E_i / T_t)
+ * over a state list (host arrays; the sum of compute_partition,
+ * exomol_functions.cpp:44-62, with its constants) for n_temps temperatures,
+ * in a fixed summation order.  Blocks until q is written. */
+int xs_partition_sum(int device, const double* energies, const int* gns, size_t n,
+                     const double* temperatures, int n_temps, double* q);
+
 /* ---- 3. manager level: BaseManager over host buffers --------------------- */
 /* kind: 0 = GpuManager (reference GPU convention), 1 = OpenMPManager
  * (reference CPU convention, computed on the GPU). */
@@ -306,7 +313,9 @@ typedef struct {
     int profile;        /* XS_VOIGT or XS_DOPPLER */
     int precision;      /* XS_FP64 or XS_MIXED */
     double temperature; /* K */
-    double partition;   /* Q(T) */
+    double partition;   /* Q(T); <= 0: from the molecule's states
+                           (xs_server_add_states), computed on the device and
+                           kept per temperature */
     double pressure;    /* atm: multiplies the molecule's gamma (given per atm)
                            and, when cut <= 0, sets the reference cut rule */
     double cut;         /* window half width in cm-1; <= 0: min(25 P, 100) for
@@ -334,6 +343,10 @@ int xs_server_add_molecule(xs_server* s, const double* nu, const double* energie
                            const double* aif, const int* gns, const double* gamma,
                            const double* n, size_t count, double mean_mass, double ref_temp,
                            int* molecule_id);
+/* Optional lower-state list of a molecule (E in cm-1, total degeneracy g),
+ * for requests that leave Q(T) to the server. */
+int xs_server_add_states(xs_server* s, int molecule_id, const double* energies, const int* gns,
+                         size_t count);
 /* Non-blocking.  XS_ERR_NOMEM when the request alone exceeds a budget. */
 int xs_server_submit(xs_server* s, const xs_request* r, unsigned long long* request_id);
 /* Blocks until the request is done (timeout_ms < 0: no limit; on timeout
