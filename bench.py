@@ -256,6 +256,15 @@ def run_ours(args, rank, world, dist):
                               warps_per_block=args.W, conditions_per_warp=args.C)
     o_f64 = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.FP64,
                               ref_temp=common["ref_temp"], conditions_per_warp=args.C64)
+    tuned = None
+    if not (args.P or args.W or args.C or args.C64) and not args.no_tune:
+        # launch shapes measured on this workload (outside the timed region)
+        tuned = {"mixed": eng.autotune(o_mix, cc, L, G, out.data_ptr(), npts)}
+        if out_f64 is not None:
+            tuned["fp64"] = eng.autotune(o_f64, cc, L, G, out_f64.data_ptr(), npts)
+            out_f64.zero_()
+        out.zero_()
+        log(f"[bench] autotuned: {tuned}")
     g_mix = eng.capture(o_mix, cc, L, G, out.data_ptr(), npts, zero_out=True)
     eng2 = g_f64 = None
     if not args.no_fp64:
@@ -433,8 +442,9 @@ def run_ours(args, rank, world, dist):
             "line_evals_per_step": pairs_step,
             "parallelism": f"{world} rank(s), independent (T,P) batches, no collective",
             "l2": "inputs larger than L2 (per-step records > 0.6 GB), no flush",
-            "points_per_thread": args.P or 4, "warps_per_block": args.W or 8,
-            "conditions_per_warp": args.C or "auto",
+            "launch_shape": tuned if tuned else {"points_per_thread": args.P or "default",
+                                                 "warps_per_block": args.W or "default",
+                                                 "conditions_per_warp": args.C or "auto"},
         },
         "accuracy_vs_fp64": {"max_rel_above_1e-6_peak": rel_max, "max_integrated_rel": integ_max},
         "fp64": {"value": f64_value, "ms_per_step": f64_step, "unit": "line-evals/s"},
@@ -717,6 +727,7 @@ def main():
     ap.add_argument("--conds", type=int, default=40, help="subset of the 40 conditions (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-serve", action="store_true", help="skip the request-server stream")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes, no autotuning")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-scale", type=float, default=1.0,

@@ -78,6 +78,12 @@ class RequestInfo(ctypes.Structure):
                 ("line_evals", ctypes.c_double), ("lines", ctypes.c_size_t)]
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [("points_per_thread", ctypes.c_int), ("warps_per_block", ctypes.c_int),
+                ("conditions_per_warp", ctypes.c_int), ("ms", ctypes.c_double),
+                ("candidates", ctypes.c_int)]
+
+
 class StreamStats(ctypes.Structure):
     _fields_ = [("total_ms", ctypes.c_double), ("copy_span_ms", ctypes.c_double),
                 ("h2d_bytes", ctypes.c_double), ("chunks", ctypes.c_int)]
@@ -116,6 +122,12 @@ _SIGS = {
     "xs_measure_peaks": (_I, [_I, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "xs_execute_noalloc": (_I, [ctypes.POINTER(Options), ctypes.POINTER(Condition),
                                 ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _VP]),
+    "xs_engine_autotune": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _I,
+                                ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _SZ,
+                                ctypes.POINTER(TuneResult)]),
+    "xs_tune_save": (_I, [ctypes.c_char_p]),
+    "xs_tune_load": (_I, [ctypes.c_char_p]),
+    "xs_tune_clear": (_I, []),
     "xs_stream_execute": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _VP, _VP,
                                _VP, _SZ, ctypes.POINTER(GridC), _VP, _SZ,
                                ctypes.POINTER(StreamStats)]),
@@ -226,6 +238,14 @@ class Engine:
         arr = (Condition * len(conds))(*conds)
         check(lib().xs_engine_execute(self.h, ctypes.byref(opts), arr, len(conds),
                                       ctypes.byref(lines), ctypes.byref(grid), out_ptr, out_stride))
+
+    def autotune(self, opts: Options, conds: list[Condition], lines: Lines, grid: GridC, out_ptr: int,
+                 out_stride: int = 0) -> dict:
+        arr = (Condition * len(conds))(*conds)
+        r = TuneResult()
+        check(lib().xs_engine_autotune(self.h, ctypes.byref(opts), arr, len(conds), ctypes.byref(lines),
+                                       ctypes.byref(grid), out_ptr, out_stride, ctypes.byref(r)))
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_}
 
     def stream_execute(self, opts: Options, cond: Condition, h_nu: int, h_s: int, h_gamma: int,
                        n: int, grid: GridC, out_ptr: int, chunk_lines: int) -> dict:

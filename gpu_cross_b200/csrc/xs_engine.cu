@@ -12,7 +12,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -83,6 +85,28 @@ void default_shape(int kind, bool mixed, int* P, int* warps) {
         *P = 1;
         *warps = 8;
     }
+}
+
+// Launch shapes chosen by xs_engine_autotune, per call signature: profile,
+// convention, precision, number of conditions, and the binary magnitudes of
+// the grid points and of the lines per grid point inside the window.
+struct Shape {
+    int P, W, C;
+    double ms;
+};
+std::mutex g_tune_mu;
+std::map<std::string, Shape> g_tune;
+
+std::string shape_key(const xs_options& o, const xs_condition* conds, int ncond, long n, int points) {
+    double cutmax = 0.0;
+    for (int c = 0; c < ncond; ++c) cutmax = std::fmax(cutmax, make_cond(o, conds[c]).cut);
+    const double win = 2.0 * cutmax / o.dfreq;
+    const double density = double(n) * win / (double(points) + win);
+    auto lg = [](double v) { return v < 1.0 ? 0 : int(std::floor(std::log2(v))); };
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), "p%d.v%d.x%d.c%d.g%d.d%d", o.profile, o.convention, o.precision,
+                  ncond < kMaxCond ? ncond : kMaxCond, lg(double(points)), lg(density));
+    return buf;
 }
 
 // Host copy of the per-condition constants.  GPU convention:
@@ -320,6 +344,17 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     if (n <= 0 || grid->points <= 0) return XS_OK;
 
     int P = opt->points_per_thread, W = opt->warps_per_block;
+    int C = opt->conditions_per_warp;
+    if (P == 0 && W == 0 && C == 0) {
+        // a shape the autotuner measured for calls like this one
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(shape_key(*opt, conds, ncond, n, grid->points));
+        if (it != g_tune.end()) {
+            P = it->second.P;
+            W = it->second.W;
+            C = it->second.C;
+        }
+    }
     {
         int dP, dW;
         default_shape(kind, mixed, &dP, &dW);
@@ -331,7 +366,6 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     if (W != 4 && W != 8) return fail(XS_ERR_INVALID, "warps_per_block must be 4 or 8");
 
     // Multi-condition tiles (Voigt batches whose conditions share the cut).
-    int C = opt->conditions_per_warp;
     if (C < 0 || C == 3 || C > 8 || (C > 4 && C != 8))
         return fail(XS_ERR_INVALID, "conditions_per_warp must be 0, 1, 2, 4 or 8");
     {
@@ -635,6 +669,103 @@ int xs_graph_destroy(xs_graph* g) {
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
     delete g;
+    return XS_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int xs_engine_autotune(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                       const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride,
+                       xs_tune_result* best) {
+    if (!e || !opt || !conds || !lines || !grid || !out || ncond < 1)
+        return fail(XS_ERR_INVALID, "xs_engine_autotune: NULL argument");
+    const int kind = opt->profile;
+    const bool mixed = kind == XS_VOIGT && opt->precision == XS_MIXED;
+    struct Cand {
+        int P, W, C;
+    };
+    std::vector<Cand> cands;
+    const int Ps[4] = {1, 2, 4, 8};
+    for (int W : {4, 8}) {
+        for (int P : Ps) {
+            if (kind != XS_VOIGT && P > 2) continue;
+            if (kind == XS_VOIGT && !mixed && P > 4) continue;
+            cands.push_back({P, W, kind == XS_VOIGT ? 1 : 0});
+        }
+        if (kind == XS_VOIGT && ncond > 1)
+            for (int C : {2, 4})
+                if (ncond % C == 0 && ncond <= kMaxCond) cands.push_back({1, W, C});
+    }
+    long n = long(lines->count);
+    if (opt->convention == XS_CONV_CPU) n = cpu_covered_lines(n, opt->cpu_threads);
+    Shape pick{0, 0, 0, 1e300};
+    for (const Cand& c : cands) {
+        xs_options o = *opt;
+        o.points_per_thread = c.P;
+        o.warps_per_block = c.W;
+        o.conditions_per_warp = c.C;
+        double ms = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {
+            int rc = xs::engine_execute(e, &o, conds, ncond, lines, grid, out, out_stride, nullptr);
+            if (rc == XS_ERR_INVALID) break;  // a shape this call cannot take (e.g. unequal cuts)
+            if (rc != XS_OK) return rc;
+            rc = xs_engine_sync(e);
+            if (rc != XS_OK) return rc;
+            double pm = 0.0, sm = 0.0;
+            rc = xs_engine_last_stats(e, &pm, &sm);
+            if (rc != XS_OK) return rc;
+            ms = pm + sm;  // the second run is the one kept (the first warms up)
+        }
+        if (ms < pick.ms) pick = Shape{c.P, c.W, c.C, ms};
+    }
+    if (pick.P == 0) return fail(XS_ERR_INVALID, "xs_engine_autotune: no launch shape fits this call");
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[shape_key(*opt, conds, ncond, n, grid->points)] = pick;
+    }
+    if (best) {
+        best->points_per_thread = pick.P;
+        best->warps_per_block = pick.W;
+        best->conditions_per_warp = pick.C;
+        best->ms = pick.ms;
+        best->candidates = int(cands.size());
+    }
+    return XS_OK;
+}
+
+int xs_tune_save(const char* path) {
+    if (!path) return fail(XS_ERR_INVALID, "xs_tune_save: NULL path");
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    FILE* f = std::fopen(path, "w");
+    if (!f) return fail(XS_ERR_INVALID, std::string("xs_tune_save: cannot write ") + path);
+    for (const auto& kv : g_tune)
+        std::fprintf(f, "%s %d %d %d %.6f\n", kv.first.c_str(), kv.second.P, kv.second.W, kv.second.C,
+                     kv.second.ms);
+    std::fclose(f);
+    return XS_OK;
+}
+
+int xs_tune_load(const char* path) {
+    if (!path) return fail(XS_ERR_INVALID, "xs_tune_load: NULL path");
+    FILE* f = std::fopen(path, "r");
+    if (!f) return fail(XS_ERR_INVALID, std::string("xs_tune_load: cannot read ") + path);
+    char key[96];
+    Shape sh{};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    while (std::fscanf(f, "%95s %d %d %d %lf", key, &sh.P, &sh.W, &sh.C, &sh.ms) == 5) {
+        const bool ok = (sh.P == 1 || sh.P == 2 || sh.P == 4 || sh.P == 8) && (sh.W == 4 || sh.W == 8) &&
+                        (sh.C == 0 || sh.C == 1 || sh.C == 2 || sh.C == 4 || sh.C == 8);
+        if (ok) g_tune[key] = sh;
+    }
+    std::fclose(f);
+    return XS_OK;
+}
+
+int xs_tune_clear(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
     return XS_OK;
 }
 

@@ -212,6 +212,26 @@ int xs_graph_destroy(xs_graph* graph);
  * denominators of the step-two kernels. */
 int xs_measure_peaks(int device, double* fp32_tflops, double* fp64_tflops, double* rcp32_tops);
 
+/* Autotuner: runs the call below once per candidate launch shape (points
+ * per thread, warps per block, conditions per warp; each twice, the second
+ * timed), keeps the fastest for calls of the same signature (profile,
+ * convention, precision, condition count, and the binary magnitudes of the
+ * grid points and of the lines per point), and reports it.  Later calls with
+ * points_per_thread = warps_per_block = conditions_per_warp = 0 use it.  `out`
+ * is accumulated into many times: clear it afterwards.  The table lives in
+ * the process; xs_tune_save / xs_tune_load keep it in a text file. */
+typedef struct {
+    int points_per_thread, warps_per_block, conditions_per_warp;
+    double ms;       /* step one + step two of the chosen shape */
+    int candidates;  /* shapes tried */
+} xs_tune_result;
+int xs_engine_autotune(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                       const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride,
+                       xs_tune_result* best);
+int xs_tune_save(const char* path);
+int xs_tune_load(const char* path);
+int xs_tune_clear(void);
+
 /* Allocation-free variant of xs_engine_execute for ONE condition.  It has no
  * counterpart in the reference.  For callers that cannot let this library
  * allocate device memory: a host whose own pool allocator already holds the

@@ -404,3 +404,32 @@ def test_graph_replay_matches_execute(engine, cuda):
             assert engine.last_stats()[1] > 0
     finally:
         g.close()
+
+
+def test_autotune_picks_a_shape_later_calls_use(engine, cuda, tmp_path):
+    import torch
+
+    lines, grid, cond = small_voigt_case(seed=21, n=2000)
+    fr = grid.freq()
+    dev = to_device(lines, cuda)
+    dfr = torch.as_tensor(fr, device=cuda)
+    out = torch.zeros(len(fr), dtype=torch.float64, device=cuda)
+    opts = capi.make_options(capi.VOIGT, grid.dfreq, cond["mean_mass"], precision=capi.MIXED)
+    cc = [capi.make_condition(cond["temperature"], cond["partition"], 1.0, 1.0, -1.0)]
+    engine.set_stream(torch.cuda.current_stream(cuda).cuda_stream)
+    capi.lib().xs_tune_clear()
+    best = engine.autotune(opts, cc, capi.make_lines(dev), capi.make_grid(dfr), out.data_ptr())
+    assert best["candidates"] >= 8 and best["ms"] > 0
+    assert best["points_per_thread"] in (1, 2, 4, 8) and best["warps_per_block"] in (4, 8)
+    auto = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, precision=capi.MIXED)
+    explicit = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, precision=capi.MIXED,
+                          P=best["points_per_thread"], W=best["warps_per_block"],
+                          C=best["conditions_per_warp"])
+    assert np.array_equal(auto, explicit)
+    path = str(tmp_path / "shapes.txt").encode()
+    capi.check(capi.lib().xs_tune_save(path))
+    capi.lib().xs_tune_clear()
+    capi.check(capi.lib().xs_tune_load(path))
+    again = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, precision=capi.MIXED)
+    assert np.array_equal(auto, again)
+    capi.lib().xs_tune_clear()
