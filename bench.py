@@ -253,9 +253,11 @@ def run_ours(args, rank, world, dist):
     G = capi.make_grid(dfr)
     o_mix = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.MIXED,
                               ref_temp=common["ref_temp"], points_per_thread=args.P,
-                              warps_per_block=args.W, conditions_per_warp=args.C)
+                              warps_per_block=args.W, conditions_per_warp=args.C,
+                              line_splits=args.S)
     o_f64 = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.FP64,
-                              ref_temp=common["ref_temp"], conditions_per_warp=args.C64)
+                              ref_temp=common["ref_temp"], conditions_per_warp=args.C64,
+                              line_splits=args.S)
     tuned = None
     if not (args.P or args.W or args.C or args.C64) and not args.no_tune:
         # launch shapes measured on this workload (outside the timed region)
@@ -720,6 +722,7 @@ def main():
     ap.add_argument("--W", type=int, default=0)
     ap.add_argument("--C", type=int, default=0, help="conditions per warp (mixed)")
     ap.add_argument("--C64", type=int, default=0, help="conditions per warp (FP64)")
+    ap.add_argument("--S", type=int, default=0, help="line splits per tile (0 = automatic)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

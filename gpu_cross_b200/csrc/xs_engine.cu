@@ -404,13 +404,14 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
                  : steptwo_blocks_per_sm(kind, opt->convention, mixed, P, W);
     if (occ < 1) occ = 1;
 
-    // Line splits.  A launch with fewer work items than resident warps
-    // (short or coarse grids over many lines) would leave most of the GPU
-    // idle while each warp walks a long line list; then each tile's lines
-    // are split into parts taken by different warps -- enough for about two
-    // waves, at least ~128 lines per part, the parts' buffer within
-    // kMaxPartBytes.  The count depends only on the call's sizes and the SM
-    // count.
+    // Line splits.  Work items are taken dynamically, but an item is a whole
+    // tile over all its lines: with fewer items than resident warps (short
+    // or coarse grids over many lines) most of the GPU idles while each warp
+    // walks a long line list, and with a few items per warp the last items
+    // leave a tail.  Each tile's lines are then split into parts taken by
+    // different warps -- enough for about 16 items per resident warp, at
+    // least ~256 lines per part, the parts' buffer within kMaxPartBytes.
+    // The count depends only on the call's sizes and the SM count.
     const int tile_pts = CG ? 32 : 32 * P;
     const int tiles = (grid->points + tile_pts - 1) / tile_pts;
     int S = opt->line_splits;
@@ -419,13 +420,13 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         const long items = long(tiles) * (CG ? group / CG : group);
         const long warps = long(occ) * W * e->num_sms;
         S = 1;
-        if (items < warps) {
+        if (items < 16 * warps) {
             double cutmax = 0.0;
             for (int c = 0; c < ncond; ++c) cutmax = std::fmax(cutmax, make_cond(*opt, conds[c]).cut);
             const double span = double(grid->points) * opt->dfreq + 2.0 * cutmax;
             const double lpt = double(n) * (double(tile_pts) * opt->dfreq + 2.0 * cutmax) / span;
-            long want = (2 * warps + items - 1) / items;
-            want = std::min<long>(want, long(lpt / 128.0));
+            long want = (16 * warps + items - 1) / items;
+            want = std::min<long>(want, long(lpt / 256.0));
             const long cap = long(kMaxPartBytes / (sizeof(double) * size_t(group) * size_t(grid->points)));
             want = std::min<long>(want, std::min<long>(cap, kMaxSplits));
             if (want > 1) S = int(want);
