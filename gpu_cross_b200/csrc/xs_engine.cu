@@ -76,11 +76,15 @@ namespace xs {
 
 int set_error(int code, const char* msg) { return fail(code, msg); }
 
-// Default launch shapes (tuned on a B200; the autotuner may override them).
-void default_shape(int kind, bool mixed, int* P, int* warps) {
+// Default launch shapes, from measurements on a B200 (the autotuner's table
+// takes precedence).  Voigt tiles of 32 P points: wide where a line's window
+// spans thousands of points (fewer partial lines per tile, record loads
+// shared by more points), narrow on coarse grids, where a 128-point tile
+// would hold mostly partial and core lines.
+void default_shape(int kind, bool mixed, double window_points, int* P, int* warps) {
     if (kind == kVoigt) {
-        *P = mixed ? 4 : 2;
-        *warps = 8;
+        *P = window_points >= 2048.0 ? 4 : (window_points >= 512.0 ? 2 : 1);
+        *warps = mixed ? 8 : 4;
     } else {
         *P = 1;
         *warps = 8;
@@ -357,7 +361,9 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     }
     {
         int dP, dW;
-        default_shape(kind, mixed, &dP, &dW);
+        double cutmax = 0.0;
+        for (int c = 0; c < ncond; ++c) cutmax = std::fmax(cutmax, make_cond(*opt, conds[c]).cut);
+        default_shape(kind, mixed, 2.0 * cutmax / opt->dfreq, &dP, &dW);
         if (P == 0) P = dP;
         if (W == 0) W = dW;
     }
