@@ -562,6 +562,11 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         if (CG) {
             sa.lsh = pa.lsh;
             sa.group = CG;
+            for (int c = 0; c < nc; ++c) {
+                const double k = 1.0 / pa.cond[c].dpw;
+                sa.kx[c] = float(k);
+                sa.kx2[c] = float(k * k);
+            }
             sa.tiles_per_cond = (grid->points + 31) / 32;
             sa.n_items = sa.tiles_per_cond * (nc / CG) * S;
         }

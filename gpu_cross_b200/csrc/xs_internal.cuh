@@ -104,6 +104,39 @@ struct __align__(16) CondRec32 {
     int core;
 };
 static_assert(sizeof(CondRec32) == 32, "CondRec32 layout");
+// Mixed-precision multi-condition layout.  The offset of grid point j from a
+// line, in Doppler widths, factors into a condition-free part and a
+// per-condition constant: the reference's gammaG = 1 / (nu dpw)
+// (cross_kernal.cu:958), so x = (nu - f_j) / (nu dpw) = X k with
+// X = (nu - f_j) / nu = (m - j) dfn + rn and k = 1 / dpw.  One X per
+// (line, point) then serves every condition of the group, and
+// u = x^2 + Cy = X^2 k^2 + Cy.
+struct __align__(16) LineShX {
+    float m;      // nearest grid index (exact below 2^24)
+    float dfn;    // df / nu
+    float rn;     // (nu - f0 - m df) / nu
+    int whole;    // 1: X from nu in FP64 and every pair of the line tested
+    int lo, hi;   // window [lo, hi) of grid indices
+    double nu;    // centre (whole lines)
+};
+static_assert(sizeof(LineShX) == 32, "LineShX layout");
+// Conditions 2k and 2k+1 of a group side by side, so that each pair of
+// values is one packed FP32x2 operand; the first two 16-byte chunks are all
+// the region-I path reads.  c15 / c55: the grid indices j of the line's
+// W4 regions II-IV (|x| + y < 15) and III-IV (< 5.5), as j - m in
+// [lo, hi] packed lo & 0xffff | hi << 16 (16-bit signed), or kCoreNone, or
+// kCoreWhole (every pair of the line classified by its FP32 x).
+struct __align__(16) CondPairX {
+    float Cy[2], D2[2];
+    float Pc[2], pref[2];
+    float y[2];
+    int c15[2];
+    int c55[2];
+    int pad[2];
+};
+static_assert(sizeof(CondPairX) == 64, "CondPairX layout");
+constexpr int kCoreNone = 1;                    // lo 1 > hi 0: empty
+constexpr int kCoreWhole = int(0x80000000u);    // lo 0 > hi -32768
 struct __align__(16) LineSh64 {
     double nu;
     int lo, hi;
@@ -162,6 +195,7 @@ struct PrepArgs {
     int group;          // > 0: multi-condition layout with this many
                         // conditions per group (Voigt only)
     void* lsh;          // multi-condition: per-line shared records per group
+                        // (LineShX mixed, LineSh64 FP64)
 };
 
 struct StepArgs {
@@ -187,6 +221,9 @@ struct StepArgs {
     int splits;
     double* part;
     size_t part_stride;
+    // Mixed multi-condition kernel: per condition k = 1 / dpw and k^2.
+    float kx[kMaxCond];
+    float kx2[kMaxCond];
 };
 
 // Kernel launchers (xs_kernels.cu).  All asynchronous on `stream`.

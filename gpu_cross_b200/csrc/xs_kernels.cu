@@ -127,8 +127,10 @@ __global__ void k_grid_check(GridDev g, unsigned* err) {
 // Step one.
 // ---------------------------------------------------------------------------
 // Returns the line's core half-width in grid points (Voigt; 0 otherwise).
+// `pair`: the mixed-precision multi-condition layout fills its condition's
+// half of a CondPairX there (k_prep_pairs stores the whole record).
 template <int KIND, int CONV, bool MIXED>
-__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c) {
+__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondPairX* pair = nullptr) {
     const CondDev& C = a.cond[c];
     const double* F = a.G.freq;
     const double f0 = F[0];
@@ -252,23 +254,64 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c) {
                 core = aa | (bb << 16);
             }
             if (MIXED) {
-                CondRec32 cr;
-                cr.ra = float(((nu_p - f0) - m * df) * g);
-                cr.dfa = float(df * g);
-                cr.Cy = float(Cy);
-                cr.D2 = float(D2);
-                cr.Pc = float(Pc);
-                cr.pref = float(pref);
-                cr.y = float(y);
-                cr.core = core;
-                reinterpret_cast<CondRec32*>(a.rec)[gi * C + cl] = cr;
+                // Region intervals: the grid indices of this chunk where
+                // |x| + y < 15 (W4 regions II-IV) and < 5.5 (III-IV), with
+                // x = (nu - f_j) g in FP64 on the analytic grid
+                // f_j = f0 + j df, so that the region of every pair is the
+                // FP64 choice (up to the grid's last-bit rounding) and never
+                // flips with the FP32 rounding of x.
+                const bool far_m = !(fabs(m) < 16000000.0);
+                int c15 = kCoreNone, c55 = kCoreNone;
+                kcl = 0;
+                if (whole) {
+                    c15 = kCoreWhole;
+                    kcl = 30000000;
+                } else {
+                    auto interval = [&](double lim, int& code) {
+                        if (!(y < lim)) return true;
+                        auto fa = [&](int j) { return fma(double(j), df, f0); };
+                        auto inside = [&](int j) { return !(fabs((nu_p - fa(j)) * g) + y >= lim); };
+                        const double hw = (lim - y) / g;
+                        const int jl = find_first(s, e, ceil((nu_p - hw - f0) / df),
+                                                  [&](int j) { return fa(j) > nu_p || inside(j); });
+                        const int jh = find_first(s, e, floor((nu_p + hw - f0) / df) + 1.0,
+                                                  [&](int j) { return fa(j) > nu_p && !inside(j); });
+                        if (jl >= jh) return true;
+                        const double rl = double(jl) - m, rh = double(jh - 1) - m;
+                        if (!(rl >= -32767.0 && rh <= 32767.0)) return false;
+                        code = int((unsigned(int(rl)) & 0xffffu) | (unsigned(int(rh)) << 16));
+                        return true;
+                    };
+                    if (interval(15.0, c15) && interval(5.5, c55)) {
+                        if (c15 != kCoreNone)
+                            kcl = max(-int(short(c15 & 0xffff)), c15 >> 16);
+                    } else {
+                        // a core wider than 32767 points: classified pair by pair
+                        c15 = kCoreWhole;
+                        kcl = 30000000;
+                    }
+                }
+                // conditions 2k, 2k+1 share one CondPairX
+                CondPairX& cp = *pair;
+                const int h = c & 1;  // groups have an even size
+                cp.Cy[h] = float(Cy);
+                cp.D2[h] = float(D2);
+                cp.Pc[h] = float(Pc);
+                cp.pref[h] = float(pref);
+                cp.y[h] = float(y);
+                cp.c15[h] = c15;
+                cp.c55[h] = c55;
+                cp.pad[h] = 0;
                 if (cl == 0) {
-                    LineSh32 ls;
-                    ls.m = float(fabs(m) < 16000000.0 ? m : 0.0);
+                    LineShX ls;
+                    ls.m = float(far_m ? 0.0 : m);
+                    ls.dfn = float(df / nu_p);
+                    ls.rn = float(((nu_p - f0) - m * df) / nu_p);
+                    ls.whole = far_m ? 1 : 0;
                     ls.lo = lo;
                     ls.hi = hi;
-                    ls.pad = 0;
-                    reinterpret_cast<LineSh32*>(a.lsh)[gi] = ls;
+                    ls.nu = nu_p;
+                    reinterpret_cast<LineShX*>(a.lsh)[gi] = ls;
                 }
             } else {
                 CondRec64 cr;
@@ -360,6 +403,40 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c) {
     a.wlo[ci] = lo;
     a.whi[ci] = hi;
     return kcl;
+}
+
+// Step one of the mixed-precision multi-condition layout: one thread per
+// (line, pair of conditions), so that each CondPairX is stored whole.
+template <int CONV>
+__global__ void __launch_bounds__(256) k_prep_pairs(PrepArgs a) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int c0 = 2 * int(blockIdx.y);
+    int k0 = 0, k1 = 0;
+    if (i < a.L.n) {
+        CondPairX cp;
+        k0 = prep_line<kVoigt, CONV, true>(a, i, c0, &cp);
+        k1 = prep_line<kVoigt, CONV, true>(a, i, c0 + 1, &cp);
+        const int C = a.group;
+        const int cg = c0 / C;
+        const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(i);
+        float4* dst = reinterpret_cast<float4*>(reinterpret_cast<CondPairX*>(a.rec) + gi * (C / 2) + (c0 - cg * C) / 2);
+        const float4* src = reinterpret_cast<const float4*>(&cp);
+#pragma unroll
+        for (int q = 0; q < int(sizeof(CondPairX) / 16); ++q) dst[q] = src[q];
+    }
+    __shared__ int smax[2][8];
+    k0 = __reduce_max_sync(0xffffffffu, k0);
+    k1 = __reduce_max_sync(0xffffffffu, k1);
+    if ((threadIdx.x & 31) == 0) {
+        smax[0][threadIdx.x >> 5] = k0;
+        smax[1][threadIdx.x >> 5] = k1;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        int m = 0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[threadIdx.x][w] > m ? smax[threadIdx.x][w] : m;
+        if (m > 0) atomicMax(a.kc + c0 + int(threadIdx.x), m);
+    }
 }
 
 template <int KIND, int CONV, bool MIXED>
@@ -523,20 +600,6 @@ __device__ __forceinline__ float w4_region3_re_f32(float x, float y) {
     const fcplx num = 16.4955f + t * (20.20933f + t * (11.96482f + t * (3.778987f + t * fcplx{.5642236f, 0.f})));
     const fcplx den = 16.4955f + t * (38.82363f + t * (39.27121f + t * (21.69274f + t * (6.699398f + t))));
     return (num.re * den.re + num.im * den.im) / (den.re * den.re + den.im * den.im);
-}
-
-// W4 region IV in FP64 (exp(U) minus a rational cancel for small y).
-__device__ double w4_region4_re(double x, double y) {
-    const cplx t = {y, -x};
-    const cplx u = t * t;
-    double sn, cs;
-    sincos(u.im, &sn, &cs);
-    const double eu = exp(u.re);
-    const cplx num =
-        36183.31 - u * (3321.9905 - u * (1540.787 - u * (219.0313 - u * (35.76683 - u * (1.320522 - u * .56419)))));
-    const cplx den =
-        32066.6 - u * (24322.84 - u * (9022.228 - u * (2186.181 - u * (364.2191 - u * (61.57037 - u * (1.841439 - u))))));
-    return eu * cs - div_re(t * num, den);
 }
 
 // W4 region IV for the mixed path: exp(U) = exp(y^2 - x^2) cos(2xy) + i(...)
@@ -1239,6 +1302,343 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
 }
 
 // ---------------------------------------------------------------------------
+// Mixed-precision multi-condition step two (Voigt), packed FP32x2.
+//
+// Work items, line runs and the fixed summation order are those of
+// k_steptwo_voigt_mc.  Per (line, point) one condition-free offset
+// X = (m - j) dfn + rn and X^2 are formed; conditions are then taken in
+// pairs, each pair one packed FP32x2 operation per step of the region-I
+// rational (u = X^2 k^2 + Cy, u^2 + D2, Pc (u + 1), accumulate), so a
+// region-I pair costs two FP32 operations and one reciprocal per condition
+// and about three issue slots in all.  Near a core, step one's region
+// intervals decide: W4 region II is evaluated in place, regions III and IV
+// are queued per warp and evaluated 32 at a time.
+// ---------------------------------------------------------------------------
+template <int C>
+struct WarpQueueX {
+    static constexpr int kCap = 32 * (C + 1);  // < 32 pending + one line's pushes
+    CoreEntry<float> q[kCap];
+    float corr[C][32];
+};
+
+// Evaluates the first k (<= 32) queued pairs (W4 regions III-IV), one per
+// lane, and adds each result to its destination lane's correction column in
+// queue order (as core_queue_flush).  Returns the new queue length.
+template <int C>
+__device__ __noinline__ int queue_flush_x(WarpQueueX<C>& cq, int qn, int k, int lane) {
+    float v = 0.0f;
+    int dest = 0;
+    if (lane < k) {
+        const CoreEntry<float> e = cq.q[lane];
+        dest = e.dest;
+        const float ax = e.x, y = e.y;
+        const float w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y)
+                                                          : w4_region4_re_mixed(ax, y);
+        v = e.pref * w;
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, dest, 1);
+    const bool start = lane < k && (lane == 0 || dest != prev + 1 || (dest & 31) == 0);
+    unsigned starts = __ballot_sync(0xffffffffu, start);
+    while (starts) {
+        const int s0 = __ffs(starts) - 1;
+        starts &= starts - 1;
+        const int e0 = starts ? __ffs(starts) - 1 : k;
+        const int d0 = __shfl_sync(0xffffffffu, dest, s0);
+        const int first = d0 & 31, row = d0 >> 5;
+        const float vv = __shfl_sync(0xffffffffu, v, (s0 + lane - first) & 31);
+        if (lane >= first && lane < first + (e0 - s0)) cq.corr[row][lane] += vv;
+    }
+    __syncwarp();
+    const int rem = qn - k;
+    for (int base = 0; base < rem; base += 32) {
+        CoreEntry<float> keep;
+        const int i = base + lane;
+        if (i < rem) keep = cq.q[k + i];
+        __syncwarp();
+        if (i < rem) cq.q[i] = keep;
+        __syncwarp();
+    }
+    return rem;
+}
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+
+// W4 region II (w4_region2_re) for two conditions at once, packed FP32x2,
+// with an approximate reciprocal for the final division.
+__device__ __forceinline__ float2 w4_region2_re_x2(float2 x, float2 y) {
+    const float a = 1.410474f, b = .5641896f, c = .75f;
+    const float2 x2 = __fmul2_rn(x, x), y2 = __fmul2_rn(y, y);
+    const float2 ur = __ffma2_rn(x2, f2s(-1.0f), y2);          // y^2 - x^2
+    const float2 nui = __fmul2_rn(__fmul2_rn(x, y), f2s(2.0f));  // -ui = 2 x y
+    const float2 nr = __ffma2_rn(ur, f2s(b), f2s(a));
+    const float2 dr = __ffma2_rn(__fmul2_rn(nui, f2s(-1.0f)), nui,
+                                 __ffma2_rn(ur, __fadd2_rn(ur, f2s(3.0f)), f2s(c)));
+    const float2 e = __ffma2_rn(ur, f2s(2.0f), f2s(3.0f));     // 3 + 2 ur
+    const float2 di = __fmul2_rn(__fmul2_rn(nui, f2s(-1.0f)), e);
+    const float2 q1 = __ffma2_rn(x2, f2s(-3.0f * b), __ffma2_rn(y2, f2s(b), f2s(a)));
+    const float2 q2 = __ffma2_rn(y2, f2s(2.0f * b), nr);
+    const float2 q3 = __fmul2_rn(__fmul2_rn(x2, f2s(2.0f)), e);
+    const float2 br = __ffma2_rn(q1, dr, __fmul2_rn(q3, q2));
+    const float2 den = __ffma2_rn(dr, dr, __fmul2_rn(di, di));
+    const float2 num = __fmul2_rn(y, br);
+    return f2(num.x * rcp_approx_f32(den.x), num.y * rcp_approx_f32(den.y));
+}
+
+template <int C, int WARPS>
+constexpr int voigt_mcx_min_blocks() {
+    return C <= 2 ? 24 / WARPS : 16 / WARPS;
+}
+
+template <int C, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>()))
+    k_steptwo_voigt_mcx(StepArgs a) {
+    static_assert(C % 2 == 0, "conditions come in pairs");
+    constexpr int NP = C / 2;
+    using Q = WarpQueueX<C>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    LineShX* lsb = reinterpret_cast<LineShX*>(smem_raw) + warp * 64;
+    CondPairX* cpb = reinterpret_cast<CondPairX*>(smem_raw + size_t(WARPS) * 64 * sizeof(LineShX)) +
+                     warp * 64 * NP;
+    Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 64 * (sizeof(LineShX) + NP * sizeof(CondPairX)))[warp];
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+#pragma unroll
+    for (int c = 0; c < C; ++c) cq.corr[c][lane] = 0.0f;
+    int qn = 0;
+    // Queues this lane's pair when `need` (x, y, pref of condition c).
+    auto push = [&](bool need, float x, float y, float pref, int c) {
+        const unsigned b = __ballot_sync(0xffffffffu, need);
+        if (need) {
+            CoreEntry<float> e;
+            e.x = x;
+            e.y = y;
+            e.pref = pref;
+            e.dest = lane | (c << 5);
+            cq.q[qn + __popc(b & lt_mask)] = e;
+        }
+        qn += __popc(b);
+    };
+
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = int(atomicAdd(a.counter, 1u));
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.n_items) break;
+        const int per_cond = a.tiles_per_cond * a.splits;
+        const int cg = item / per_cond;
+        const int tile = (item - cg * per_cond) / a.splits;
+        const int split = item - cg * per_cond - tile * a.splits;
+        const int t0 = a.G.start + tile * 32;
+        const int end = a.G.start + a.G.points;
+        const int t1 = t0 + 32 < end ? t0 + 32 : end;
+        const int tl = t1 - 1;
+        const size_t gbase = size_t(cg) * size_t(a.n);
+        const int* whi = a.whi + gbase;
+        const int* wlo = a.wlo + gbase;
+        const int* mi = a.mi;
+        int kc = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) kc = max(kc, a.kc[cg * C + c]);
+        // line indices fit 32 bits (at most 2^31 - 1 lines per call)
+        const int La = int(warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; }));
+        const int Lb = int(warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; }));
+        const int fs = int(warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; }));
+        const int Cb = int(warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; }));
+        const int fe = Cb > fs ? Cb : fs;
+        const int E = int(warp_lower_bound(La, Lb, lane, [&](long i) { return mi[i] >= t0 - kc; }));
+        const int Fc = int(warp_lower_bound(E, Lb, lane, [&](long i) { return mi[i] > tl + kc; }));
+        const LineShX* lsh = reinterpret_cast<const LineShX*>(a.lsh) + gbase;
+        const CondPairX* cpr = reinterpret_cast<const CondPairX*>(a.rec) + gbase * NP;
+
+        const int jj = t0 + lane;
+        const float jf = float(jj);
+        const double fj = a.G.freq[jj < t1 ? jj : tl];
+        float kx[C];
+        float2 k2[NP];
+        float2 acc[NP], sum[NP], cmp[NP];
+#pragma unroll
+        for (int c = 0; c < C; ++c) kx[c] = a.kx[cg * C + c];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            k2[p] = f2(a.kx2[cg * C + 2 * p], a.kx2[cg * C + 2 * p + 1]);
+            acc[p] = sum[p] = cmp[p] = f2(0.0f, 0.0f);
+        }
+
+        // Region I of one pair of conditions: u = X^2 k^2 + Cy,
+        // acc += Pc (u + 1) / (u^2 + D2).  Pairs where `keep` is false add
+        // exactly zero: the reciprocal is replaced by 0 (not multiplied by a
+        // mask, so that an infinite reciprocal of a skipped pair never
+        // reaches the sum); with GUARD the product itself is selected, for
+        // lines whose u may overflow.
+        auto region1 = [&](auto guard, float X2, const CondPairX& r, int p, bool keep0, bool keep1) {
+            const float4 f0 = *reinterpret_cast<const float4*>(&r.Cy[0]);
+            const float4 f1 = *reinterpret_cast<const float4*>(&r.Pc[0]);
+            const float2 u = __ffma2_rn(f2(X2, X2), k2[p], f2(f0.x, f0.y));
+            const float2 den = __ffma2_rn(u, u, f2(f0.z, f0.w));
+            const float2 num = __ffma2_rn(u, f2(f1.x, f1.y), f2(f1.x, f1.y));
+            const float2 rr = f2(keep0 ? rcp_approx_f32(den.x) : 0.0f, keep1 ? rcp_approx_f32(den.y) : 0.0f);
+            if constexpr (decltype(guard)::value) {
+                acc[p].x += keep0 ? num.x * rr.x : 0.0f;
+                acc[p].y += keep1 ? num.y * rr.y : 0.0f;
+            } else {
+                acc[p] = __ffma2_rn(num, rr, acc[p]);
+            }
+        };
+        const std::false_type plain;
+        const std::true_type guarded;
+
+        const int ngroups = split_groups(Lb - La, a.splits, split);
+        auto gstart = [&](int gi) { return La + 32 * (split + gi * a.splits); };
+        auto stage_group = [&](int bufi, int b, int cnt) {
+            stage(lsb + bufi * 32, lsh + b, cnt, lane);
+            stage(cpb + bufi * 32 * NP, cpr + size_t(b) * NP, cnt * NP, lane);
+        };
+        if (ngroups > 0) {
+            const int b = gstart(0);
+            stage_group(0, b, Lb - b < 32 ? Lb - b : 32);
+            cp_async_commit();
+        }
+        for (int gi = 0; gi < ngroups; ++gi) {
+            if (gi + 1 < ngroups) {
+                const int b = gstart(gi + 1);
+                const int rem = Lb - b;
+                stage_group((gi + 1) & 1, b, rem < 32 ? rem : 32);
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncwarp();
+            const LineShX* SL = lsb + (gi & 1) * 32;
+            const CondPairX* SC = cpb + (gi & 1) * 32 * NP;
+            const int gb = gstart(gi);
+            const int ge = Lb - gb < 32 ? Lb : gb + 32;
+            auto lo_of = [&](int v) { return (v < gb ? gb : (v > ge ? ge : v)) - gb; };
+            const int a0 = lo_of(La), a1 = lo_of(fs), b1 = lo_of(E), c1 = lo_of(Fc), d1 = lo_of(fe),
+                      e1 = lo_of(Lb);
+            // Full lines away from every core: region I with no test.
+            auto fast_run = [&](int x, int y) {
+#pragma unroll 2
+                for (int t = x; t < y; ++t) {
+                    const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
+                    const float X = fmaf(s.x - jf, s.y, s.z);
+                    const float X2 = X * X;
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, true, true);
+                }
+            };
+            // Partial lines away from every core: the window as a lane mask.
+            auto masked_run = [&](int x, int y) {
+                for (int t = x; t < y; ++t) {
+                    const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
+                    const bool in = jj >= SL[t].lo && jj < SL[t].hi && jj < t1;
+                    const float X = fmaf(s.x - jf, s.y, s.z);
+                    const float X2 = X * X;
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, in, in);
+                }
+            };
+            // Core candidates.  Per condition whose region interval reaches
+            // the row: pairs with |x| + y < 15 drop out of region I; region
+            // II is evaluated in place for both conditions of the pair at
+            // once, regions III and IV are queued.
+            auto cand_run = [&](int x, int y) {
+                for (int t = x; t < y; ++t) {
+                    const LineShX s = SL[t];
+                    const bool full = (t >= a1 && t < d1);
+                    const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
+                    const float X = s.whole ? float((s.nu - fj) / s.nu) : fmaf(s.m - jf, s.dfn, s.rn);
+                    const float X2 = X * X;
+                    const float aX = fabsf(X);
+                    const int mline = int(s.m);
+                    const int rel = jj - mline;
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+                        const CondPairX& r = SC[t * NP + p];
+                        bool keep[2], r2[2], deep[2], queue[2];
+                        float ax[2];
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int c15 = r.c15[h];
+                            keep[h] = in;
+                            r2[h] = deep[h] = queue[h] = false;
+                            ax[h] = aX * kx[2 * p + h];
+                            if (c15 == kCoreWhole) {
+                                const float sx = ax[h] + r.y[h];
+                                const bool i15 = sx < 15.0f, i55 = sx < 5.5f;
+                                // beyond x ~ 1e9 region I is taken as 0
+                                keep[h] = in && !i15 && ax[h] < 1.0e9f;
+                                r2[h] = in && i15 && !i55;
+                                deep[h] = in && i55;
+                                queue[h] = true;
+                            } else if (c15 != kCoreNone) {
+                                const int lo = int(short(c15 & 0xffff)), hi = c15 >> 16;
+                                if (lo <= tl - mline && hi >= t0 - mline) {
+                                    const int c55 = r.c55[h];
+                                    const int lo5 = int(short(c55 & 0xffff)), hi5 = c55 >> 16;
+                                    const bool i15 = rel >= lo && rel <= hi;
+                                    const bool i55 = rel >= lo5 && rel <= hi5;  // kCoreNone: empty
+                                    keep[h] = in && !i15;
+                                    r2[h] = in && i15 && !i55;
+                                    deep[h] = in && i55;
+                                    queue[h] = lo5 <= tl - mline && hi5 >= t0 - mline;
+                                }
+                            }
+                        }
+                        region1(guarded, X2, r, p, keep[0], keep[1]);
+                        if (__any_sync(0xffffffffu, r2[0] || r2[1])) {
+                            const float2 w = w4_region2_re_x2(f2(ax[0], ax[1]), f2(r.y[0], r.y[1]));
+                            acc[p].x += r2[0] ? r.pref[0] * w.x : 0.0f;
+                            acc[p].y += r2[1] ? r.pref[1] * w.y : 0.0f;
+                        }
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+                            if (queue[h]) push(deep[h], ax[h], r.y[h], r.pref[h], 2 * p + h);
+                    }
+                    __syncwarp();
+                    while (qn >= 32) qn = queue_flush_x<C>(cq, qn, 32, lane);
+                }
+            };
+            fast_run(a1, min(d1, b1));
+            fast_run(max(a1, c1), d1);
+            masked_run(a0, min(a1, b1));
+            masked_run(max(a0, c1), a1);
+            masked_run(d1, min(e1, b1));
+            masked_run(max(d1, c1), e1);
+            cand_run(b1, c1);
+            // Pending core pairs, then the compensated (Kahan) fold of this
+            // group's FP32 partials.
+            while (qn > 0) qn = queue_flush_x<C>(cq, qn, qn < 32 ? qn : 32, lane);
+            auto kahan = [](float part, float& sm, float& cm) {
+                const float yk = part - cm;
+                const float tk = sm + yk;
+                cm = (tk - sm) - yk;
+                sm = tk;
+            };
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                kahan(acc[p].x + cq.corr[2 * p][lane], sum[p].x, cmp[p].x);
+                kahan(acc[p].y + cq.corr[2 * p + 1][lane], sum[p].y, cmp[p].y);
+                cq.corr[2 * p][lane] = 0.0f;
+                cq.corr[2 * p + 1][lane] = 0.0f;
+                acc[p] = f2(0.0f, 0.0f);
+            }
+            __syncwarp();
+        }
+        if (jj < t1) {
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                put_result(a, cg * C + 2 * p, split, jj, double(sum[p].x) - double(cmp[p].x));
+                put_result(a, cg * C + 2 * p + 1, split, jj, double(sum[p].y) - double(cmp[p].y));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Step two, Doppler and Gaussian (bin-integrated erf differences, FP64).
 // ---------------------------------------------------------------------------
 template <int KIND, int CONV, int P, int WARPS>
@@ -1379,12 +1779,37 @@ cudaError_t run_voigt_mc(int blocks, const StepArgs& a, cudaStream_t st, int* oc
     return cudaGetLastError();
 }
 
+template <int C, int WARPS>
+cudaError_t run_voigt_mcx(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
+    const size_t smem = size_t(WARPS) * (64 * (sizeof(LineShX) + (C / 2) * sizeof(CondPairX)) +
+                                         sizeof(WarpQueueX<C>));
+    if (smem > 48 * 1024) {
+        if (cudaFuncSetAttribute(k_steptwo_voigt_mcx<C, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem)) != cudaSuccess)
+            return cudaGetLastError();
+    }
+    if (occ) {
+        *occ = blocks_per_sm(k_steptwo_voigt_mcx<C, WARPS>, WARPS * 32, smem);
+        return cudaSuccess;
+    }
+    k_steptwo_voigt_mcx<C, WARPS><<<blocks, WARPS * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
 template <int WARPS, bool MIXED>
 cudaError_t dispatch_mc_c(int C, int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
+    if (MIXED) {
+        switch (C) {
+            case 2: return run_voigt_mcx<2, WARPS>(blocks, a, st, occ);
+            case 4: return run_voigt_mcx<4, WARPS>(blocks, a, st, occ);
+            case 8: return run_voigt_mcx<8, WARPS>(blocks, a, st, occ);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (C) {
-        case 2: return run_voigt_mc<2, WARPS, MIXED>(blocks, a, st, occ);
-        case 4: return run_voigt_mc<4, WARPS, MIXED>(blocks, a, st, occ);
-        case 8: return run_voigt_mc<8, WARPS, MIXED>(blocks, a, st, occ);
+        case 2: return run_voigt_mc<2, WARPS, false>(blocks, a, st, occ);
+        case 4: return run_voigt_mc<4, WARPS, false>(blocks, a, st, occ);
+        case 8: return run_voigt_mc<8, WARPS, false>(blocks, a, st, occ);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1471,7 +1896,11 @@ cudaError_t launch_reduce_splits(const StepArgs& a, int ncond_out, cudaStream_t 
 cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaStream_t stream) {
     if (a.L.n <= 0 || a.ncond <= 0) return cudaSuccess;
     const dim3 grid(unsigned((a.L.n + 255) / 256), unsigned(a.ncond));
-    if (kind == kVoigt) {
+    if (kind == kVoigt && mixed && a.group > 0) {
+        const dim3 pgrid(grid.x, unsigned(a.ncond / 2));
+        if (conv == kConvGpu) k_prep_pairs<kConvGpu><<<pgrid, 256, 0, stream>>>(a);
+        else k_prep_pairs<kConvCpu><<<pgrid, 256, 0, stream>>>(a);
+    } else if (kind == kVoigt) {
         if (conv == kConvGpu) {
             if (mixed) k_prep<kVoigt, kConvGpu, true><<<grid, 256, 0, stream>>>(a);
             else k_prep<kVoigt, kConvGpu, false><<<grid, 256, 0, stream>>>(a);
@@ -1525,7 +1954,7 @@ size_t record_bytes(int kind, bool mixed) {
 ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off, int group) {
     auto al = [](size_t v) { return (v + 255) / 256 * 256; };
     ScratchPlan p;
-    const size_t rec = group > 0 ? (mixed ? sizeof(CondRec32) : sizeof(CondRec64))
+    const size_t rec = group > 0 ? (mixed ? sizeof(CondPairX) / 2 : sizeof(CondRec64))
                                  : record_bytes(kind, mixed);
     const size_t nwin = group > 0 ? size_t((ncond + group - 1) / group) : size_t(ncond);
     p.off_rec = al(base_off);
@@ -1534,7 +1963,8 @@ ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_
     p.off_mi = al(p.off_whi + sizeof(int) * n * nwin);
     p.off_kc = al(p.off_mi + sizeof(int) * n);
     p.off_lsh = al(p.off_kc + sizeof(int) * size_t(kMaxCond));
-    p.need = al(p.off_lsh + (group > 0 ? sizeof(LineSh32) * n * nwin : 0));
+    const size_t lsh = mixed ? sizeof(LineShX) : sizeof(LineSh64);
+    p.need = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
     return p;
 }
 

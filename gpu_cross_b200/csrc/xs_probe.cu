@@ -49,9 +49,11 @@ __global__ void k_rcp32(float* sink, float seed) {
     for (int i = 0; i < kIters / 4; ++i) {
 #pragma unroll
         for (int c = 0; c < kChains; ++c) {
+            // a <- 1/a + 1 (converges to the golden ratio): the add keeps
+            // consecutive reciprocals from cancelling
             float r;
             asm volatile("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a[c]));
-            a[c] = r;
+            a[c] = r + 1.0f;
         }
     }
     float s = 0.f;

@@ -209,6 +209,43 @@ def test_multi_condition_tiles_vs_oracle(engine, cuda, C):
         assert_mixed_parity(mix[k], f64[k])
 
 
+@pytest.mark.parametrize("C", [2, 4])
+def test_multi_condition_mixed_edges(engine, cuda, C):
+    """Mixed multi-condition tiles against FP64 where the region intervals
+    are clipped or replaced: lines centred beyond both grid ends, a grid
+    chunk that starts inside the grid, and a grid fine enough (1e-6 cm-1)
+    that the cores span more than 2^15 points and lines 20 cm-1 away lie
+    more than 2^24 points from the grid's first point (pair-by-pair
+    classification, offsets from the FP64 centre)."""
+    base = dict(mean_mass=17.03, pressure=1.0, ref_temp=296.0)
+    conds = [dict(base, temperature=t, partition=synth.partition_poly(t), gamma_scale=p, cut=25.0)
+             for t in (300.0, 2100.0) for p in (1e-3, 1.0)]
+    # 0.1 cm-1 grid; lines on both sides of it and across both ends
+    lines = synth.random_lines(2000, 960.0, 1140.0, 2500.0, 1e-6, 1e2, seed=61, pressure_atm=1.0)
+    grid = synth.Grid(990.0, 1110.0, 1200)
+    fr = grid.freq()
+    for start, points in ((0, None), (317, 611)):
+        f64 = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, C=C,
+                         start_idx=start, points=points)
+        mix = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, C=C,
+                         start_idx=start, points=points, precision=capi.MIXED)
+        for k in range(len(conds)):
+            assert_mixed_parity(mix[k], f64[k])
+    # 1e-6 cm-1 grid over 0.05 cm-1: cores of +-0.2 cm-1 (2e5 points); the
+    # lines at 1020 cm-1 reach it through the 25 cm-1 cut from 2e7 points away
+    near = synth.random_lines(60, 999.98, 1000.07, 2500.0, 1e-3, 1e2, seed=62, pressure_atm=1.0)
+    far = synth.random_lines(20, 1020.0, 1020.5, 2500.0, 1e-3, 1e2, seed=63, pressure_atm=1.0)
+    both = synth.LineList(*(np.concatenate([getattr(near, f), getattr(far, f)])
+                            for f in ("nu", "energies", "aif", "gns", "gamma", "n")))
+    fine = synth.Grid(1000.0, 1000.05, 50001)
+    ff = fine.freq()
+    f64 = run_engine(engine, capi.VOIGT, both, ff, base, fine.dfreq, cuda, conds=conds, C=C)
+    mix = run_engine(engine, capi.VOIGT, both, ff, base, fine.dfreq, cuda, conds=conds, C=C,
+                     precision=capi.MIXED)
+    for k in range(len(conds)):
+        assert_mixed_parity(mix[k], f64[k])
+
+
 def test_empty_and_outside_lines(engine, cuda):
     lines, grid, cond = small_voigt_case(seed=2, n=100)
     fr = grid.freq()
