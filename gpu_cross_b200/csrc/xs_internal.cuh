@@ -90,20 +90,6 @@ static_assert(sizeof(RecV32) == 64, "RecV32 layout");
 // (same cut) is evaluated together, one 32-point row of the grid per warp
 // and C accumulators per lane.  What the conditions share is stored once per
 // line; the rest once per (line, condition), conditions innermost.
-// core packs the core band around m: (m - clo) | (chi - m) << 16, each part
-// at most 0x7fff (0x7fff: unbounded); -1: no core band.
-struct __align__(16) LineSh32 {
-    float m;
-    int lo, hi;
-    int pad;
-};
-static_assert(sizeof(LineSh32) == 16, "LineSh32 layout");
-struct __align__(16) CondRec32 {
-    float ra, dfa, Cy, D2;
-    float Pc, pref, y;
-    int core;
-};
-static_assert(sizeof(CondRec32) == 32, "CondRec32 layout");
 // Mixed-precision multi-condition layout.  The offset of grid point j from a
 // line, in Doppler widths, factors into a condition-free part and a
 // per-condition constant: the reference's gammaG = 1 / (nu dpw)
@@ -137,6 +123,8 @@ struct __align__(16) CondPairX {
 static_assert(sizeof(CondPairX) == 64, "CondPairX layout");
 constexpr int kCoreNone = 1;                    // lo 1 > hi 0: empty
 constexpr int kCoreWhole = int(0x80000000u);    // lo 0 > hi -32768
+// FP64: core packs the core band around m: (m - clo) | (chi - m) << 16, each
+// part at most 0x7fff (0x7fff: unbounded); -1: no core band.
 struct __align__(16) LineSh64 {
     double nu;
     int lo, hi;
@@ -208,7 +196,7 @@ struct StepArgs {
     double* out;
     size_t out_stride;  // elements between conditions
     GridDev G;
-    const void* lsh;    // multi-condition layout (see LineSh32)
+    const void* lsh;    // multi-condition layout (LineShX mixed, LineSh64 FP64)
     int group;          // conditions per group (multi-condition kernel)
     int tiles_per_cond;
     int n_items;

@@ -1079,41 +1079,32 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
     }
 }
 
-// Multi-condition step two: a work item is (group of C conditions that share
-// one window, row of 32 grid points); each lane owns one grid point and C
-// accumulators.  The line runs are found as in k_steptwo_voigt (windows and
+// Multi-condition step two, FP64: a work item is (group of C conditions that
+// share one window, row of 32 grid points); each lane owns one grid point and
+// C accumulators.  The line runs are found as in k_steptwo_voigt (windows and
 // grid indices are shared by the group; the core run uses the group's widest
 // core), and every line loads its shared record once and one small record
 // per condition.
-template <int C, int WARPS, bool MIXED>
-constexpr int voigt_mc_min_blocks() {
-    return MIXED ? 24 / WARPS : 1;
-}
-
-template <int C, int WARPS, bool MIXED>
-__global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIXED>()))
-    k_steptwo_voigt_mc(StepArgs a) {
-    using CR = typename std::conditional<MIXED, CondRec32, CondRec64>::type;
-    using LS = typename std::conditional<MIXED, LineSh32, LineSh64>::type;
-    using T = typename std::conditional<MIXED, float, double>::type;
-    using Q = WarpCoreQueue<C, MIXED>;
+template <int C, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt_mc(StepArgs a) {
+    using Q = WarpCoreQueue<C, false>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    LS* lsb = reinterpret_cast<LS*>(smem_raw) + warp * 64;
-    CR* crb = reinterpret_cast<CR*>(smem_raw + size_t(WARPS) * 64 * sizeof(LS)) + warp * 64 * C;
-    Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 64 * (sizeof(LS) + C * sizeof(CR)))[warp];
+    LineSh64* lsb = reinterpret_cast<LineSh64*>(smem_raw) + warp * 64;
+    CondRec64* crb = reinterpret_cast<CondRec64*>(smem_raw + size_t(WARPS) * 64 * sizeof(LineSh64)) + warp * 64 * C;
+    Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 64 * (sizeof(LineSh64) + C * sizeof(CondRec64)))[warp];
     const double* F = a.G.freq;
     const unsigned lt_mask = (1u << lane) - 1u;
 
 #pragma unroll
-    for (int c = 0; c < C; ++c) cq.corr[c][lane] = T(0);
+    for (int c = 0; c < C; ++c) cq.corr[c][lane] = 0.0;
     int qn = 0;
-    auto push = [&](bool need, T x, T y, T pref, int c) {
+    auto push = [&](bool need, double x, double y, double pref, int c) {
         const unsigned b = __ballot_sync(0xffffffffu, need);
         if (b == 0u) return;
         if (need) {
-            CoreEntry<T> e;
+            CoreEntry<double> e;
             e.x = x;
             e.y = y;
             e.pref = pref;
@@ -1153,63 +1144,42 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
         // only lines in [E, Fc) can have a core band that reaches the row
         const long E = warp_lower_bound(La, Lb, lane, [&](long i) { return mi[i] >= t0 - kc; });
         const long Fc = warp_lower_bound(E, Lb, lane, [&](long i) { return mi[i] > tl + kc; });
-        const LS* lsh = reinterpret_cast<const LS*>(a.lsh) + gbase;
-        const CR* crec = reinterpret_cast<const CR*>(a.rec) + gbase * C;
+        const LineSh64* lsh = reinterpret_cast<const LineSh64*>(a.lsh) + gbase;
+        const CondRec64* crec = reinterpret_cast<const CondRec64*>(a.rec) + gbase * C;
 
         const int jj = t0 + lane;
-        const float jf = float(jj);
-        const double fj = MIXED ? 0.0 : F[jj < t1 ? jj : tl];
-        float accf[C], sumf[C], cmpf[C];
+        const double fj = F[jj < t1 ? jj : tl];
         double accd[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-            accf[c] = sumf[c] = cmpf[c] = 0.0f;
-            accd[c] = 0.0;
-        }
+        for (int c = 0; c < C; ++c) accd[c] = 0.0;
 
         // x (in Doppler widths) of this lane's point for condition record r.
-        auto offset = [&](const LS& s, const CR& r) -> T {
-            if constexpr (MIXED) return T(fmaf(float(s.m) - jf, float(r.dfa), float(r.ra)));
-            else return T((double(s.nu) - fj) * double(r.g));
-        };
-        auto region1 = [&](T xs, const CR& r, T mask, int c) {
-            if (MIXED) {
-                const float u = fmaf(float(xs), float(xs), float(r.Cy));
-                accf[c] = fmaf(fmaf(u, float(r.Pc), float(r.Pc)),
-                               rcp_approx_f32(fmaf(u, u, float(r.D2))) * float(mask), accf[c]);
-            } else {
-                const double u = fma(double(xs), double(xs), double(r.Cy));
-                accd[c] = fma(fma(u, double(r.Pc), double(r.Pc)),
-                              rcp_refined_f64(fma(u, u, double(r.D2))) * double(mask), accd[c]);
-            }
+        auto offset = [&](const LineSh64& s, const CondRec64& r) { return (s.nu - fj) * r.g; };
+        auto region1 = [&](double xs, const CondRec64& r, double mask, int c) {
+            const double u = fma(xs, xs, r.Cy);
+            accd[c] = fma(fma(u, r.Pc, r.Pc), rcp_refined_f64(fma(u, u, r.D2)) * mask, accd[c]);
         };
         // One condition of a partial line, or of a line whose core band may
         // reach this row; `in`: this lane's point lies in the line's window.
-        auto core_cond = [&](const LS& s, const CR& r, int mline, bool in, int c) {
-            const T xs = offset(s, r);
-            const T ax = xs < T(0) ? -xs : xs;
-            const T sx = ax + T(r.y);
+        auto core_cond = [&](const LineSh64& s, const CondRec64& r, int mline, bool in, int c) {
+            const double xs = offset(s, r);
+            const double ax = xs < 0.0 ? -xs : xs;
+            const double sx = ax + r.y;
             bool band = false;
             if (r.core != -1) {
                 const int aa = r.core & 0xffff, bb = (r.core >> 16) & 0xffff;
                 const int rel = jj - mline;
                 band = (aa == 0x7fff || rel >= -aa) && (bb == 0x7fff || rel <= bb);
             }
-            // x and y of the FP64 path are bit-identical to the reference's,
-            // so |x| + y < 15 is the reference's region choice there.
-            const bool special = in && band && sx < T(15);
+            // x and y are bit-identical to the reference's, so |x| + y < 15
+            // is the reference's region choice.
+            const bool special = in && band && sx < 15.0;
             if (!__any_sync(0xffffffffu, special)) {
-                region1(xs, r, in ? T(1) : T(0), c);
+                region1(xs, r, in ? 1.0 : 0.0, c);
                 return;
             }
-            const bool r2 = MIXED && special && sx >= T(5.5);
-            const bool deep = special && !r2;
-            region1(xs, r, (in && !special) ? T(1) : T(0), c);
-            if (MIXED) {
-                if (__any_sync(0xffffffffu, r2) && r2)
-                    accf[c] += float(r.pref) * w4_region2_re<float>(float(ax), float(r.y));
-            }
-            push(deep, ax, T(r.y), T(r.pref), c);
+            region1(xs, r, (in && !special) ? 1.0 : 0.0, c);
+            push(special, ax, r.y, r.pref, c);
         };
 
         // this item's groups of 32 lines: gi-th starts at La + 32 (s + gi S)
@@ -1235,8 +1205,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
                 cp_async_wait<0>();
             }
             __syncwarp();
-            const LS* SL = lsb + (gi & 1) * 32;
-            const CR* SC = crb + (gi & 1) * 32 * C;
+            const LineSh64* SL = lsb + (gi & 1) * 32;
+            const CondRec64* SC = crb + (gi & 1) * 32 * C;
             const long gb = gstart(gi);
             const long ge = Lb - gb < 32 ? Lb : gb + 32;
             auto lo_of = [&](long v) { return int((v < gb ? gb : (v > ge ? ge : v)) - gb); };
@@ -1247,17 +1217,17 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
             // Full lines away from every core: region I with no test.
             auto fast_run = [&](int x, int y) {
                 for (int t = x; t < y; ++t) {
-                    const LS s = SL[t];
+                    const LineSh64 s = SL[t];
 #pragma unroll
-                    for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], T(1), c);
+                    for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], 1.0, c);
                 }
             };
             // Partial lines away from every core: region I, the window as a
             // lane mask.
             auto masked_run = [&](int x, int y) {
                 for (int t = x; t < y; ++t) {
-                    const LS s = SL[t];
-                    const T mask = (jj >= s.lo && jj < s.hi && jj < t1) ? T(1) : T(0);
+                    const LineSh64 s = SL[t];
+                    const double mask = (jj >= s.lo && jj < s.hi && jj < t1) ? 1.0 : 0.0;
 #pragma unroll
                     for (int c = 0; c < C; ++c) region1(offset(s, SC[t * C + c]), SC[t * C + c], mask, c);
                 }
@@ -1267,17 +1237,15 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
             // lane-by-lane core path.
             auto cand_run = [&](int x, int y) {
                 for (int t = x; t < y; ++t) {
-                    const LS s = SL[t];
+                    const LineSh64 s = SL[t];
                     const bool full = (t >= a1 && t < d1);
                     const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
-                    const T mask = in ? T(1) : T(0);
-                    int mline;
-                    if constexpr (MIXED) mline = int(s.m);  // exact below 2^24; "whole" lines have unbounded bands
-                    else mline = mi[gb + t];
+                    const double mask = in ? 1.0 : 0.0;
+                    const int mline = mi[gb + t];
                     bool any_core = false;
 #pragma unroll
                     for (int c = 0; c < C; ++c) {
-                        const CR& r = SC[t * C + c];
+                        const CondRec64& r = SC[t * C + c];
                         bool hit = false;
                         if (r.core != -1) {
                             const int aa = r.core & 0xffff, bb = (r.core >> 16) & 0xffff;
@@ -1291,7 +1259,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
                         }
                     }
                     if (any_core)
-                        while (qn >= 32) qn = core_queue_flush<C, MIXED>(cq, qn, 32, lane);
+                        while (qn >= 32) qn = core_queue_flush<C, false>(cq, qn, 32, lane);
                 }
             };
             fast_run(a1, min(d1, b1));
@@ -1301,36 +1269,18 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mc_min_blocks<C, WARPS, MIX
             masked_run(d1, min(e1, b1));
             masked_run(max(d1, c1), e1);
             cand_run(b1, c1);
-            if (MIXED) {
-                if (qn > 0) qn = core_queue_flush<C, MIXED>(cq, qn, qn, lane);
-#pragma unroll
-                for (int c = 0; c < C; ++c) {
-                    const float part = accf[c] + float(cq.corr[c][lane]);
-                    cq.corr[c][lane] = T(0);
-                    const float yk = part - cmpf[c];
-                    const float tk = sumf[c] + yk;
-                    cmpf[c] = (tk - sumf[c]) - yk;
-                    sumf[c] = tk;
-                    accf[c] = 0.0f;
-                }
-            }
             __syncwarp();
         }
-        if (!MIXED) {
-            while (qn > 0) qn = core_queue_flush<C, MIXED>(cq, qn, qn < 32 ? qn : 32, lane);
+        while (qn > 0) qn = core_queue_flush<C, false>(cq, qn, qn < 32 ? qn : 32, lane);
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                accd[c] += double(cq.corr[c][lane]);
-                cq.corr[c][lane] = T(0);
-            }
-            __syncwarp();
+        for (int c = 0; c < C; ++c) {
+            accd[c] += cq.corr[c][lane];
+            cq.corr[c][lane] = 0.0;
         }
+        __syncwarp();
         if (jj < t1) {
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const double v = MIXED ? double(sumf[c]) - double(cmpf[c]) : accd[c];
-                put_result(a, cg * C + c, split, jj, v);
-            }
+            for (int c = 0; c < C; ++c) put_result(a, cg * C + c, split, jj, accd[c]);
         }
     }
 }
@@ -1793,21 +1743,20 @@ cudaError_t run_voigt(int blocks, const StepArgs& a, cudaStream_t st, int* occ) 
     return cudaGetLastError();
 }
 
-template <int C, int WARPS, bool MIXED>
+template <int C, int WARPS>
 cudaError_t run_voigt_mc(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
-    using CR = typename std::conditional<MIXED, CondRec32, CondRec64>::type;
-    using LS = typename std::conditional<MIXED, LineSh32, LineSh64>::type;
-    const size_t smem = size_t(WARPS) * (64 * (sizeof(LS) + C * sizeof(CR)) + sizeof(WarpCoreQueue<C, MIXED>));
+    const size_t smem = size_t(WARPS) * (64 * (sizeof(LineSh64) + C * sizeof(CondRec64)) +
+                                         sizeof(WarpCoreQueue<C, false>));
     if (smem > 48 * 1024) {
-        if (cudaFuncSetAttribute(k_steptwo_voigt_mc<C, WARPS, MIXED>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        if (cudaFuncSetAttribute(k_steptwo_voigt_mc<C, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem)) != cudaSuccess)
             return cudaGetLastError();
     }
     if (occ) {
-        *occ = blocks_per_sm(k_steptwo_voigt_mc<C, WARPS, MIXED>, WARPS * 32, smem);
+        *occ = blocks_per_sm(k_steptwo_voigt_mc<C, WARPS>, WARPS * 32, smem);
         return cudaSuccess;
     }
-    k_steptwo_voigt_mc<C, WARPS, MIXED><<<blocks, WARPS * 32, smem, st>>>(a);
+    k_steptwo_voigt_mc<C, WARPS><<<blocks, WARPS * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -1839,9 +1788,9 @@ cudaError_t dispatch_mc_c(int C, int blocks, const StepArgs& a, cudaStream_t st,
         }
     }
     switch (C) {
-        case 2: return run_voigt_mc<2, WARPS, false>(blocks, a, st, occ);
-        case 4: return run_voigt_mc<4, WARPS, false>(blocks, a, st, occ);
-        case 8: return run_voigt_mc<8, WARPS, false>(blocks, a, st, occ);
+        case 2: return run_voigt_mc<2, WARPS>(blocks, a, st, occ);
+        case 4: return run_voigt_mc<4, WARPS>(blocks, a, st, occ);
+        case 8: return run_voigt_mc<8, WARPS>(blocks, a, st, occ);
         default: return cudaErrorInvalidValue;
     }
 }
