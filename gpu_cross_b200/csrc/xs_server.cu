@@ -9,13 +9,15 @@
 //   * admits queued requests (FIFO) while their device and pinned-host
 //     memory fit the budgets, giving each a lane (stream + engine) and
 //     filling its grid and zeroing its output on that stream;
-//   * issues chunks to every lane that has room, the request with the least
-//     remaining work first, so small requests that arrive while a large one
-//     runs are interleaved between its chunks and finish early;
+//   * issues chunks, at most as many in flight as there are lanes: each
+//     time the request with the least remaining work over all lanes (its
+//     lane having room), so small requests that arrive while a large one
+//     runs are interleaved between its chunks and finish early, and a large
+//     one runs at the GPU's full rate when nothing smaller waits;
 //   * after a request's last chunk, copies its result to pinned host memory
 //     and, when that copy's event completes, releases its memory and wakes
 //     the waiter.
-// Work from different lanes overlaps on the device.  A request's chunks
+// Work from different lanes may overlap on the device.  A request's chunks
 // depend only on the request itself, so its result is bit-identical whether
 // it runs alone or in a mix.
 #include <cuda_runtime.h>
@@ -542,13 +544,20 @@ void scheduler(xs_server* s) {
             progress = true;
         }
         s->n_queued = int(s->queue.size());
-        // issue: per lane, the admitted request with the least remaining work
-        for (size_t li = 0; li < s->lanes.size(); ++li) {
-            Lane& ln = s->lanes[li];
-            while (int(ln.flight.size()) < depth) {
+        // issue: the admitted request with the least remaining work over all
+        // lanes (its own lane having room), while fewer chunks than lanes
+        // are in flight.  Step-two kernels fill the GPU, so chunks of
+        // different lanes mostly run one after the other: choosing over all
+        // lanes lets a large request run at the GPU's full rate when nothing
+        // smaller waits, instead of sharing it with the other lanes' work.
+        {
+            int total = 0;
+            for (const Lane& ln : s->lanes) total += int(ln.flight.size());
+            const int cap = int(s->lanes.size());
+            while (total < cap) {
                 Request* best = nullptr;
                 for (Request* r : s->active)
-                    if (r->lane == int(li) && r->next < r->chunks.size() &&
+                    if (r->next < r->chunks.size() && int(s->lanes[size_t(r->lane)].flight.size()) < depth &&
                         (!best || r->remaining < best->remaining))
                         best = r;
                 if (!best) break;
@@ -557,6 +566,7 @@ void scheduler(xs_server* s) {
                     fail_all(s, std::string("launch failed: ") + xs_last_error());
                     return;
                 }
+                ++total;
                 progress = true;
             }
         }

@@ -313,8 +313,9 @@ int xs_manager_get_ntrans(xs_manager* m, size_t* ntrans);
  * their memory fits the budgets.  Each request's grid is split into chunks
  * of whole 256-point tiles with bounded work; a scheduler thread interleaves
  * the chunks of all admitted requests over several streams (the request
- * with the least remaining work first), so a request that arrives while a
- * large one runs does not wait for all of it.  A request's chunks depend
+ * with the least remaining work over all streams first, as many chunks in
+ * flight as there are streams), so a request that arrives while a large one
+ * runs does not wait for all of it.  A request's chunks depend
  * only on the request, so its result is the same alone and in any mix. */
 typedef struct xs_server xs_server;
 
