@@ -464,7 +464,7 @@ def run_ours(args, rank, world, dist):
         "e2e": {"value": e2e_value, "unit": "line-evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "serving": serving,
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": g_mix.kernel_count() * args.steps,
         "clocks": clk,
         "when": datetime.datetime.now(datetime.timezone.utc).isoformat(),
     }
@@ -523,7 +523,7 @@ def run_doppler(args, rank, world, dist):
             out_host.copy_(out, non_blocking=True)
         s1.record(stream)
         torch.cuda.synchronize(dev)
-        res[cut] = dict(pairs=pairs, ms=ms, e2e_ms=s0.elapsed_time(s1) / 2)
+        res[cut] = dict(pairs=pairs, ms=ms, e2e_ms=s0.elapsed_time(s1) / 2, kernels=g.kernel_count())
         g.close()
     eng.close()
     # the reference OpenMPManager (unmodified: cut 100) on a slice, and the
@@ -575,7 +575,7 @@ def run_doppler(args, rank, world, dist):
                 "d2h_bytes_per_step": int(grid.npoints * 8)},
         "note": ("pairs beyond ~6 Doppler widths add exactly 0 in FP64 and are skipped, so the "
                  "line-evals/s counts the reference window, most of which needs no work"),
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": res[25.0]["kernels"] * args.steps,
         "when": datetime.datetime.now(datetime.timezone.utc).isoformat(),
     }
 
@@ -686,7 +686,7 @@ def run_stream(args, rank, world, dist):
         "e2e": {"value": pairs * world / (e2e_ms * 1e-3), "unit": "line-evals/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(grid.npoints * 8),
                 "ms_per_step": e2e_ms},
-        "gpu_launches": None,
+        "gpu_launches": int(sum(st["kernels"] for st in st_list)),
         "clocks": clk,
         "when": datetime.datetime.now(datetime.timezone.utc).isoformat(),
     }

@@ -86,7 +86,7 @@ class TuneResult(ctypes.Structure):
 
 class StreamStats(ctypes.Structure):
     _fields_ = [("total_ms", ctypes.c_double), ("copy_span_ms", ctypes.c_double),
-                ("h2d_bytes", ctypes.c_double), ("chunks", ctypes.c_int)]
+                ("h2d_bytes", ctypes.c_double), ("chunks", ctypes.c_int), ("kernels", ctypes.c_int)]
 
 
 _VP = ctypes.c_void_p
@@ -118,6 +118,7 @@ _SIGS = {
                                ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _SZ, _I,
                                ctypes.POINTER(_VP)]),
     "xs_graph_launch": (_I, [_VP, _VP]),
+    "xs_graph_kernel_count": (_I, [_VP, ctypes.POINTER(ctypes.c_int)]),
     "xs_graph_destroy": (_I, [_VP]),
     "xs_measure_peaks": (_I, [_I, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "xs_execute_noalloc": (_I, [ctypes.POINTER(Options), ctypes.POINTER(Condition),
@@ -280,6 +281,12 @@ class Graph:
 
     def launch(self, stream_handle: int | None = None) -> None:
         check(lib().xs_graph_launch(self.h, stream_handle))
+
+    def kernel_count(self) -> int:
+        """Kernel launches one replay makes."""
+        k = ctypes.c_int()
+        check(lib().xs_graph_kernel_count(self.h, ctypes.byref(k)))
+        return int(k.value)
 
     def close(self) -> None:
         if self.h:

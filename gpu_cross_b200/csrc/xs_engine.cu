@@ -499,6 +499,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     const unsigned ev_flags = (cap == cudaStreamCaptureStatusActive) ? cudaEventRecordExternal : 0u;
     cudaError_t err = launch_grid_check(G, words, st);
     if (err != cudaSuccess) return cuda_fail(err, "grid check launch");
+    int launched = G.npoints_total >= 2 ? 1 : 0;
 
     for (int c0 = 0; c0 < ncond; c0 += group) {
         const int nc = std::min(group, ncond - c0);
@@ -535,6 +536,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         if (err != cudaSuccess) return cuda_fail(err, "core-width reset");
         err = launch_prep(kind, opt->convention, mixed, pa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step one launch");
+        ++launched;
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[1], st, ev_flags);
 
         StepArgs sa;
@@ -575,13 +577,16 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         err = CG ? launch_steptwo_mc(mixed, CG, W, blocks, sa, st)
                 : launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step two launch");
+        if (blocks > 0 && sa.n_items > 0) ++launched;
         err = launch_reduce_splits(sa, nc, st);
         if (err != cudaSuccess) return cuda_fail(err, "split reduction launch");
+        if (S > 1) ++launched;
         if (timing && c0 + nc >= ncond) {
             cudaEventRecordWithFlags(e->ev[2], st, ev_flags);
             e->timed = true;
         }
     }
+    if (ov) ov->kernels += launched;
     return XS_OK;
 }
 
@@ -672,6 +677,22 @@ int xs_graph_launch(xs_graph* g, void* stream) {
     if (!g) return fail(XS_ERR_INVALID, "xs_graph_launch: NULL graph");
     DeviceGuard dg(g->e->device);
     XS_CU(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+    return XS_OK;
+}
+
+int xs_graph_kernel_count(const xs_graph* g, int* kernels) {
+    if (!g || !kernels) return fail(XS_ERR_INVALID, "xs_graph_kernel_count: NULL argument");
+    size_t n = 0;
+    XS_CU(cudaGraphGetNodes(g->graph, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n > 0) XS_CU(cudaGraphGetNodes(g->graph, nodes.data(), &n));
+    int k = 0;
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType t;
+        XS_CU(cudaGraphNodeGetType(node, &t));
+        if (t == cudaGraphNodeTypeKernel) ++k;
+    }
+    *kernels = k;
     return XS_OK;
 }
 

@@ -22,6 +22,7 @@ struct ExecOverride {
     double beta = 0.0;            //   the cross_section_data the caller copied)
     const float* s32 = nullptr;   // streamed Voigt lines: S(T) and gamma(T, P)
     const float* gl32 = nullptr;  //   per line (see LinesDev)
+    mutable int kernels = 0;      // out: kernels the call launched (added to)
 };
 
 int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,

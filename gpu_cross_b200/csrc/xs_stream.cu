@@ -117,6 +117,7 @@ extern "C" int xs_stream_execute(xs_engine* e, const xs_options* opt, const xs_c
     cudaEventRecord(B.t0, es);
     cudaEventRecord(B.c0, B.cs);
     const size_t nchunks = (n + cl - 1) / cl;
+    int kernels = 0;
     for (size_t k = 0; k < nchunks; ++k) {
         const int b = int(k & 1);
         const size_t off = k * cl;
@@ -145,6 +146,7 @@ extern "C" int xs_stream_execute(xs_engine* e, const xs_options* opt, const xs_c
             ov.gl32 = B.gl[b];
             const int rc = xs::engine_execute(e, opt, cond, 1, &L, &G, out, 0, &ov);
             if (rc != XS_OK) return rc;
+            kernels += ov.kernels;
         }
         err = cudaEventRecord(B.done[b], es);
         if (err != cudaSuccess) return st_fail(XS_ERR_CUDA, cudaGetErrorString(err));
@@ -164,6 +166,7 @@ extern "C" int xs_stream_execute(xs_engine* e, const xs_options* opt, const xs_c
         stats->copy_span_ms = cms;
         stats->h2d_bytes = double(n) * (sizeof(double) + 2 * sizeof(float));
         stats->chunks = int(nchunks);
+        stats->kernels = kernels;
     }
     return XS_OK;
 }

@@ -205,6 +205,8 @@ int xs_engine_capture(xs_engine* e, const xs_options* opt, const xs_condition* c
                       const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride,
                       int zero_out, xs_graph** graph);
 int xs_graph_launch(xs_graph* graph, void* stream);
+/* Kernel launches one replay of the graph makes (its kernel nodes). */
+int xs_graph_kernel_count(const xs_graph* graph, int* kernels);
 int xs_graph_destroy(xs_graph* graph);
 
 /* Measured throughput of this device's FP32 FMA and FP64 FMA pipes
@@ -271,6 +273,7 @@ typedef struct {
     double copy_span_ms;  /* first copy issued -> last copy done */
     double h2d_bytes;
     int chunks;
+    int kernels;          /* kernels launched */
 } xs_stream_stats;
 int xs_stream_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond,
                       const double* h_nu, const float* h_s, const float* h_gamma, size_t n,
