@@ -77,6 +77,41 @@ def pairs_gpu_window(nu: np.ndarray, freq: np.ndarray, cut: float) -> int:
     return int(np.sum(hi - lo))
 
 
+def region_histogram(lines, grid, conds, common, stride: int = 50) -> dict:
+    """Share of the window's (line, point) pairs in each W4 region, from every
+    stride-th line: region I |x| + y >= 15, II >= 5.5, III y >= 0.195|x| - 0.176,
+    IV the rest, with x = (nu - f) / (nu dpw) and y = gamma(T, P) / (nu dpw)
+    as the GPU convention computes them (counted per line from the half-widths
+    of each region in grid points)."""
+    kb, c, na = 1.380658e-16, 2.99792458e10, 6.0221412927e23
+    nu = lines.nu[::stride]
+    gam, nex = lines.gamma[::stride], lines.n[::stride]
+    fr = grid.freq()
+    f0, df, npts = fr[0], grid.dfreq, grid.npoints
+
+    def count(h):  # grid points with |nu - f| < h
+        lo = np.clip(np.floor((nu - h - f0) / df) + 1, 0, npts)
+        hi = np.clip(np.ceil((nu + h - f0) / df) - 1, -1, npts - 1)
+        return np.maximum(hi - lo + 1, 0).sum()
+
+    tot = {"I": 0.0, "II": 0.0, "III": 0.0, "IV": 0.0}
+    for cd in conds:
+        t = cd["temperature"]
+        g = 1.0 / (nu * np.sqrt(2.0 * kb * t * na / common["mean_mass"]) / c)
+        y = gam * cd["pressure_atm"] * (common["ref_temp"] / t) ** nex * g
+        win = pairs_gpu_window(nu, fr, cd["cut"])
+        n15 = count(np.maximum(15.0 - y, 0.0) / g)
+        n55 = count(np.maximum(5.5 - y, 0.0) / g)
+        # region III: |x| <= (y + 0.176) / 0.195 inside |x| < 5.5 - y
+        n3 = count(np.clip(np.minimum(5.5 - y, (y + 0.176) / 0.195), 0.0, None) / g)
+        tot["I"] += win - n15
+        tot["II"] += n15 - n55
+        tot["III"] += n3
+        tot["IV"] += n55 - n3
+    s = sum(tot.values())
+    return {k: v / s for k, v in tot.items()} if s > 0 else tot
+
+
 def pairs_cpu_window(nu: np.ndarray, f0: float, df: float, npts: int, cut: float) -> int:
     """Pairs of the reference OpenMPManager window
     [round((nu-cut-f0)/df), round((nu+cut-f0)/df)) clamped to the grid."""
@@ -373,13 +408,16 @@ def run_ours(args, rank, world, dist):
 
     step2_ms = float(np.mean(step2))
     achieved = pairs_step * FLOPS_PER_PAIR / (step2_ms * 1e-3) / 1e12
-    traffic = None
+    traffic = xu_pct = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("steptwo_mixed_sweep_bytes_per_launch")
+            tj = json.load(open(tpath))
+            traffic = tj.get("steptwo_mixed_sweep_bytes_per_launch")
+            xu_pct = tj.get("steptwo_mixed_sweep_xu_pipe_pct")
         except (OSError, ValueError):
             traffic = None
+    regions = region_histogram(lines, grid, conds, common) if args.workload == "sweep" else None
 
     # the reference's own GPU kernels (cross_kernal.cu built for sm_100a) on a
     # bounded sample: one condition, a nu-slice of the list, chunked the way
@@ -458,6 +496,8 @@ def run_ours(args, rank, world, dist):
             "peak_source": "measured (in-repo FP32 FMA probe, xs_measure_peaks, burst)",
             "flops_per_pair": FLOPS_PER_PAIR,
             "other_peaks": peaks,
+            "region_share": regions,
+            "xu_pipe_pct_ncu": xu_pct if args.workload == "sweep" else None,
         },
         "cpu_baseline": cpu,
         "reference_gpu_kernel": ref_gpu,
