@@ -659,7 +659,8 @@ struct CoreEntry {
 template <int P, bool MIXED>
 struct WarpCoreQueue {
     using T = typename std::conditional<MIXED, float, double>::type;
-    static constexpr int kCap = 32 * (P + 1);  // < 32 left + up to P rows of 32
+    static constexpr int kCap = 32 * (P + 1);  // < 32 left + up to P rows of 32 (rows of
+                                               // points, or conditions)
     CoreEntry<T> q[kCap];
     T corr[P][32];
 };
@@ -1298,54 +1299,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt_mc(StepArgs a) {
 // intervals decide: W4 region II is evaluated in place, regions III and IV
 // are queued per warp and evaluated 32 at a time.
 // ---------------------------------------------------------------------------
-template <int C>
-struct WarpQueueX {
-    static constexpr int kCap = 32 * (C + 1);  // < 32 pending + one line's pushes
-    CoreEntry<float> q[kCap];
-    float corr[C][32];
-};
-
-// Evaluates the first k (<= 32) queued pairs (W4 regions III-IV), one per
-// lane, and adds each result to its destination lane's correction column in
-// queue order (as core_queue_flush).  Returns the new queue length.
-template <int C>
-__device__ __noinline__ int queue_flush_x(WarpQueueX<C>& cq, int qn, int k, int lane) {
-    float v = 0.0f;
-    int dest = 0;
-    if (lane < k) {
-        const CoreEntry<float> e = cq.q[lane];
-        dest = e.dest;
-        const float ax = e.x, y = e.y;
-        const float w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y)
-                                                          : w4_region4_re_f32(ax, y);
-        v = e.pref * w;
-    }
-    const int prev = __shfl_up_sync(0xffffffffu, dest, 1);
-    const bool start = lane < k && (lane == 0 || dest != prev + 1 || (dest & 31) == 0);
-    unsigned starts = __ballot_sync(0xffffffffu, start);
-    while (starts) {
-        const int s0 = __ffs(starts) - 1;
-        starts &= starts - 1;
-        const int e0 = starts ? __ffs(starts) - 1 : k;
-        const int d0 = __shfl_sync(0xffffffffu, dest, s0);
-        const int first = d0 & 31, row = d0 >> 5;
-        const float vv = __shfl_sync(0xffffffffu, v, (s0 + lane - first) & 31);
-        if (lane >= first && lane < first + (e0 - s0)) cq.corr[row][lane] += vv;
-    }
-    __syncwarp();
-    const int rem = qn - k;
-    for (int base = 0; base < rem; base += 32) {
-        CoreEntry<float> keep;
-        const int i = base + lane;
-        if (i < rem) keep = cq.q[k + i];
-        __syncwarp();
-        if (i < rem) cq.q[i] = keep;
-        __syncwarp();
-    }
-    return rem;
-}
-
-
 // W4 region II (w4_region2_re) for two conditions at once, packed FP32x2,
 // with an approximate reciprocal for the final division.
 __device__ __forceinline__ float2 w4_region2_re_x2(float2 x, float2 y) {
@@ -1377,7 +1330,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
     k_steptwo_voigt_mcx(StepArgs a) {
     static_assert(C % 2 == 0, "conditions come in pairs");
     constexpr int NP = C / 2;
-    using Q = WarpQueueX<C>;
+    using Q = WarpCoreQueue<C, true>;  // one row per condition
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -1581,7 +1534,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                             if (queue[h]) push(deep[h], ax[h], r.y[h], r.pref[h], 2 * p + h);
                     }
                     __syncwarp();
-                    while (qn >= 32) qn = queue_flush_x<C>(cq, qn, 32, lane);
+                    while (qn >= 32) qn = core_queue_flush<C, true>(cq, qn, 32, lane);
                 }
             };
             fast_run(a1, min(d1, b1));
@@ -1593,7 +1546,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             cand_run(b1, c1);
             // Pending core pairs, then the compensated (Kahan) fold of this
             // group's FP32 partials.
-            while (qn > 0) qn = queue_flush_x<C>(cq, qn, qn < 32 ? qn : 32, lane);
+            while (qn > 0) qn = core_queue_flush<C, true>(cq, qn, qn < 32 ? qn : 32, lane);
             auto kahan = [](float part, float& sm, float& cm) {
                 const float yk = part - cm;
                 const float tk = sm + yk;
@@ -1763,7 +1716,7 @@ cudaError_t run_voigt_mc(int blocks, const StepArgs& a, cudaStream_t st, int* oc
 template <int C, int WARPS>
 cudaError_t run_voigt_mcx(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
     const size_t smem = size_t(WARPS) * (64 * (sizeof(LineShX) + (C / 2) * sizeof(CondPairX)) +
-                                         sizeof(WarpQueueX<C>));
+                                         sizeof(WarpCoreQueue<C, true>));
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(k_steptwo_voigt_mcx<C, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)) != cudaSuccess)
