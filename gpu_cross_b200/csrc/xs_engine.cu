@@ -374,13 +374,34 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     // Multi-condition tiles (Voigt batches whose conditions share the cut).
     if (C < 0 || C == 3 || C > 8 || (C > 4 && C != 8))
         return fail(XS_ERR_INVALID, "conditions_per_warp must be 0, 1, 2, 4 or 8");
+    // Order in which the conditions are evaluated (their results still go to
+    // their own rows).  Voigt: by cut, then by decreasing Lorentz-to-Doppler
+    // ratio (the gamma scale times (T_ref/T)^0.6, over the Doppler width per
+    // unit wavenumber), so that the conditions sharing a multi-condition
+    // group have similar core widths: a group's core run is set by its
+    // widest core, and conditions whose y exceeds 15 have none.
+    std::vector<int> order(static_cast<size_t>(ncond));
+    for (int c = 0; c < ncond; ++c) order[size_t(c)] = c;
+    if (kind == XS_VOIGT) {
+        std::vector<double> cutv(order.size()), yv(order.size());
+        for (int c = 0; c < ncond; ++c) {
+            const CondDev d = make_cond(*opt, conds[c]);
+            cutv[size_t(c)] = d.cut;
+            const double yc = d.gamma_scale * std::pow(d.tratio, 0.6) / d.dpw;
+            yv[size_t(c)] = std::isfinite(yc) ? yc : 0.0;
+        }
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            if (cutv[size_t(x)] != cutv[size_t(y)]) return cutv[size_t(x)] < cutv[size_t(y)];
+            return yv[size_t(x)] > yv[size_t(y)];
+        });
+    }
     {
         auto groups_ok = [&](int cg) {
             if (cg < 2 || ncond > kMaxCond || ncond % cg != 0) return false;
             for (int g0 = 0; g0 < ncond; g0 += cg) {
-                const double cut0 = make_cond(*opt, conds[g0]).cut;
+                const double cut0 = make_cond(*opt, conds[order[size_t(g0)]]).cut;
                 for (int k = 1; k < cg; ++k)
-                    if (make_cond(*opt, conds[g0 + k]).cut != cut0) return false;
+                    if (make_cond(*opt, conds[order[size_t(g0 + k)]]).cut != cut0) return false;
             }
             return true;
         };
@@ -392,8 +413,8 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
             // path is faster with one condition and 32*P points per warp.
             C = (mixed && groups_ok(2)) ? 2 : 1;
         } else if (C > 1 && !groups_ok(C)) {
-            return fail(XS_ERR_INVALID, "conditions_per_warp needs ncond <= 64, a multiple of it, "
-                                        "and equal cuts within each group");
+            return fail(XS_ERR_INVALID, "conditions_per_warp needs ncond <= 64 and, for every cut, a "
+                                        "number of conditions that is a multiple of it");
         }
     }
     const int CG = C > 1 ? C : 0;
@@ -509,7 +530,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.G = G;
         pa.ncond = nc;
         for (int c = 0; c < nc; ++c) {
-            pa.cond[c] = make_cond(*opt, conds[c0 + c]);
+            pa.cond[c] = make_cond(*opt, conds[order[size_t(c0 + c)]]);
             if (ov && ov->use_consts) {
                 pa.cond[c].cmcoef = ov->cmcoef;
                 pa.cond[c].beta = ov->beta;
@@ -547,8 +568,9 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         sa.mi = pa.mi;
         sa.kc = pa.kc;
         sa.n = n;
-        sa.out = out + size_t(c0) * out_stride;
+        sa.out = out;
         sa.out_stride = out_stride;
+        for (int c = 0; c < nc; ++c) sa.row[c] = order[size_t(c0 + c)];
         sa.G = G;
         sa.tiles_per_cond = (grid->points + 32 * P - 1) / (32 * P);
         sa.n_items = sa.tiles_per_cond * nc * S;

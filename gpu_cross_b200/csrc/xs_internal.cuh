@@ -212,6 +212,9 @@ struct StepArgs {
     // Mixed multi-condition kernel: per condition k = 1 / dpw and k^2.
     float kx[kMaxCond];
     float kx2[kMaxCond];
+    // Output row of each condition of the launch: its sums go to
+    // out + row[c] * out_stride.
+    int row[kMaxCond];
 };
 
 // Kernel launchers (xs_kernels.cu).  All asynchronous on `stream`.
@@ -220,7 +223,7 @@ cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaS
 // P = points per thread (1, 2, 4, 8), warps per block (4 or 8).
 cudaError_t launch_steptwo(int kind, int conv, bool mixed, int P, int warps, int blocks,
                            const StepArgs& a, cudaStream_t stream);
-// out[c][G.start + j] += sum over s of part[(c * splits + s) * stride + j].
+// out[row[c]][G.start + j] += sum over s of part[(c * splits + s) * stride + j].
 cudaError_t launch_reduce_splits(const StepArgs& a, int ncond_out, cudaStream_t stream);
 // Resident blocks per SM for a step-two configuration.
 int steptwo_blocks_per_sm(int kind, int conv, bool mixed, int P, int warps);

@@ -544,7 +544,7 @@ __device__ __forceinline__ int split_groups(long nl, int splits, int s) {
 // its part when the tile is split.
 __device__ __forceinline__ void put_result(const StepArgs& a, int c, int s, int j, double v) {
     if (a.splits <= 1)
-        a.out[size_t(c) * a.out_stride + size_t(j)] += v;
+        a.out[size_t(a.row[c]) * a.out_stride + size_t(j)] += v;
     else
         a.part[(size_t(c) * a.splits + s) * a.part_stride + size_t(j - a.G.start)] = v;
 }
@@ -1668,7 +1668,7 @@ __global__ void k_reduce_splits(StepArgs a, int ncond_out) {
     const double* p = a.part + size_t(c) * a.splits * a.part_stride + size_t(j);
     double v = 0.0;
     for (int s = 0; s < a.splits; ++s) v += p[size_t(s) * a.part_stride];
-    a.out[size_t(c) * a.out_stride + size_t(a.G.start + j)] += v;
+    a.out[size_t(a.row[c]) * a.out_stride + size_t(a.G.start + j)] += v;
 }
 
 template <class K>
