@@ -551,6 +551,8 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.mixed_tile_span = CG ? 32 : 32 * P;
         pa.group = CG;
         pa.lsh = base + plan.off_lsh;
+        pa.civ = reinterpret_cast<CoreIv*>(base + plan.off_civ);
+        pa.cyp = reinterpret_cast<float2*>(base + plan.off_cyp);
 
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, ev_flags);
         err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(kMaxCond), st);
@@ -603,6 +605,29 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         err = launch_reduce_splits(sa, nc, st);
         if (err != cudaSuccess) return cuda_fail(err, "split reduction launch");
         if (S > 1) ++launched;
+        if (CG && mixed) {
+            // the pairs inside the lines' region intervals (W4 regions II-IV)
+            CoreArgs ca;
+            std::memset(&ca, 0, sizeof(ca));
+            ca.civ = pa.civ;
+            ca.cyp = pa.cyp;
+            ca.lsh = static_cast<const LineShX*>(pa.lsh);
+            ca.mi = pa.mi;
+            ca.kc = pa.kc;
+            ca.freq = G.freq;
+            ca.n = n;
+            ca.group = CG;
+            ca.G = G;
+            ca.out = out;
+            ca.out_stride = out_stride;
+            for (int c = 0; c < nc; ++c) {
+                ca.kx[c] = sa.kx[c];
+                ca.row[c] = sa.row[c];
+            }
+            err = launch_core_mcx(ca, nc, st);
+            if (err != cudaSuccess) return cuda_fail(err, "core pass launch");
+            ++launched;
+        }
         if (timing && c0 + nc >= ncond) {
             cudaEventRecordWithFlags(e->ev[2], st, ev_flags);
             e->timed = true;

@@ -108,21 +108,24 @@ struct __align__(16) LineShX {
 static_assert(sizeof(LineShX) == 32, "LineShX layout");
 // Conditions 2k and 2k+1 of a group side by side, so that each pair of
 // values is one packed FP32x2 operand; the first two 16-byte chunks are all
-// the region-I path reads.  c15 / c55: the grid indices j of the line's
-// W4 regions II-IV (|x| + y < 15) and III-IV (< 5.5), as j - m in
-// [lo, hi] packed lo & 0xffff | hi << 16 (16-bit signed), or kCoreNone, or
-// kCoreWhole (every pair of the line classified by its FP32 x).
+// the region-I path reads.  lo / hi: the grid indices [lo, hi] of the chunk
+// where the line's |x| + y < 15 (W4 regions II-IV; empty: lo > hi); step two
+// leaves those pairs to the core pass.
 struct __align__(16) CondPairX {
     float Cy[2], D2[2];
-    float Pc[2], pref[2];
-    float y[2];
-    int c15[2];
-    int c55[2];
+    float Pc[2];
+    int lo[2];
+    int hi[2];
     int pad[2];
 };
-static_assert(sizeof(CondPairX) == 64, "CondPairX layout");
-constexpr int kCoreNone = 1;                    // lo 1 > hi 0: empty
-constexpr int kCoreWhole = int(0x80000000u);    // lo 0 > hi -32768
+static_assert(sizeof(CondPairX) == 48, "CondPairX layout");
+// Per (line, condition) of the mixed multi-condition layout, for the core
+// pass: the grid indices of W4 regions II-IV [lo15, hi15] and III-IV
+// [lo55, hi55] (empty: lo > hi) inside the line's window.
+struct __align__(16) CoreIv {
+    int lo15, hi15, lo55, hi55;
+};
+static_assert(sizeof(CoreIv) == 16, "CoreIv layout");
 // FP64: core packs the core band around m: (m - clo) | (chi - m) << 16, each
 // part at most 0x7fff (0x7fff: unbounded); -1: no core band.
 struct __align__(16) LineSh64 {
@@ -184,6 +187,8 @@ struct PrepArgs {
                         // conditions per group (Voigt only)
     void* lsh;          // multi-condition: per-line shared records per group
                         // (LineShX mixed, LineSh64 FP64)
+    CoreIv* civ;        // mixed multi-condition: region intervals and
+    float2* cyp;        //   (y, pref) per (condition, line), condition-major
 };
 
 struct StepArgs {
@@ -233,10 +238,30 @@ size_t record_bytes(int kind, bool mixed);
 // `ncond` conditions of `n` lines, the per-line grid index and the
 // per-condition core widths; sections 256-byte aligned from `base_off`.
 struct ScratchPlan {
-    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, need;
+    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, need;
 };
 ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off,
                          int group = 0);
+
+// Core pass of the mixed multi-condition layout: for every (condition, row
+// of 32 grid points), the W4 regions II-IV of the pairs inside the lines'
+// region intervals, added to out + row[c] * out_stride in line order.
+struct CoreArgs {
+    const CoreIv* civ;
+    const float2* cyp;
+    const LineShX* lsh;
+    const int* mi;
+    const int* kc;
+    const double* freq;
+    long n;             // lines per condition
+    int group;          // conditions per group (LineShX is per group)
+    GridDev G;
+    double* out;
+    size_t out_stride;
+    float kx[kMaxCond];  // 1 / dpw
+    int row[kMaxCond];
+};
+cudaError_t launch_core_mcx(const CoreArgs& a, int ncond, cudaStream_t stream);
 
 // Multi-condition step two (Voigt): C conditions per warp, 32 points per warp.
 cudaError_t launch_steptwo_mc(bool mixed, int C, int warps, int blocks, const StepArgs& a,

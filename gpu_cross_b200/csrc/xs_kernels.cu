@@ -254,53 +254,53 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
                 core = aa | (bb << 16);
             }
             if (MIXED) {
-                // Region intervals: the grid indices of this chunk where
-                // |x| + y < 15 (W4 regions II-IV) and < 5.5 (III-IV), with
-                // x = (nu - f_j) g in FP64 on the analytic grid
+                // Region intervals: the grid indices of the line's window
+                // where |x| + y < 15 (W4 regions II-IV) and < 5.5 (III-IV),
+                // with x = (nu - f_j) g in FP64 on the analytic grid
                 // f_j = f0 + j df, so that the region of every pair is the
                 // FP64 choice (up to the grid's last-bit rounding) and never
-                // flips with the FP32 rounding of x.
+                // flips with the FP32 rounding of x.  Step two leaves the
+                // pairs of [lo15, hi15] to the core pass.
                 const bool far_m = !(fabs(m) < 16000000.0);
-                int c15 = kCoreNone, c55 = kCoreNone;
-                kcl = 0;
+                auto interval = [&](double lim, int& jlo, int& jhi) {
+                    jlo = 1;
+                    jhi = 0;
+                    if (!(y < lim) || lo >= hi) return;
+                    auto fa = [&](int j) { return fma(double(j), df, f0); };
+                    auto inside = [&](int j) { return !(fabs((nu_p - fa(j)) * g) + y >= lim); };
+                    const double hw = (lim - y) / g;
+                    const int jl = find_first(lo, hi, ceil((nu_p - hw - f0) / df),
+                                              [&](int j) { return fa(j) > nu_p || inside(j); });
+                    const int jh = find_first(lo, hi, floor((nu_p + hw - f0) / df) + 1.0,
+                                              [&](int j) { return fa(j) > nu_p && !inside(j); });
+                    if (jl < jh) {
+                        jlo = jl;
+                        jhi = jh - 1;
+                    }
+                };
+                CoreIv iv;
+                interval(15.0, iv.lo15, iv.hi15);
+                interval(5.5, iv.lo55, iv.hi55);
                 if (whole) {
-                    c15 = kCoreWhole;
-                    kcl = 30000000;
+                    kcl = 30000000;  // every tile takes the line as a core candidate
                 } else {
-                    auto interval = [&](double lim, int& code) {
-                        if (!(y < lim)) return true;
-                        auto fa = [&](int j) { return fma(double(j), df, f0); };
-                        auto inside = [&](int j) { return !(fabs((nu_p - fa(j)) * g) + y >= lim); };
-                        const double hw = (lim - y) / g;
-                        const int jl = find_first(s, e, ceil((nu_p - hw - f0) / df),
-                                                  [&](int j) { return fa(j) > nu_p || inside(j); });
-                        const int jh = find_first(s, e, floor((nu_p + hw - f0) / df) + 1.0,
-                                                  [&](int j) { return fa(j) > nu_p && !inside(j); });
-                        if (jl >= jh) return true;
-                        const double rl = double(jl) - m, rh = double(jh - 1) - m;
-                        if (!(rl >= -32767.0 && rh <= 32767.0)) return false;
-                        code = int((unsigned(int(rl)) & 0xffffu) | (unsigned(int(rh)) << 16));
-                        return true;
-                    };
-                    if (interval(15.0, c15) && interval(5.5, c55)) {
-                        if (c15 != kCoreNone)
-                            kcl = max(-int(short(c15 & 0xffff)), c15 >> 16);
-                    } else {
-                        // a core wider than 32767 points: classified pair by pair
-                        c15 = kCoreWhole;
-                        kcl = 30000000;
+                    kcl = 0;
+                    if (iv.lo15 <= iv.hi15) {
+                        const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
+                        kcl = w < 3.0e7 ? int(w) : 30000000;
                     }
                 }
+                const size_t ci2 = size_t(c) * size_t(a.L.n) + size_t(i);
+                a.civ[ci2] = iv;
+                a.cyp[ci2] = make_float2(float(y), float(pref));
                 // conditions 2k, 2k+1 share one CondPairX
                 CondPairX& cp = *pair;
                 const int h = c & 1;  // groups have an even size
                 cp.Cy[h] = float(Cy);
                 cp.D2[h] = float(D2);
                 cp.Pc[h] = float(Pc);
-                cp.pref[h] = float(pref);
-                cp.y[h] = float(y);
-                cp.c15[h] = c15;
-                cp.c55[h] = c55;
+                cp.lo[h] = iv.lo15;
+                cp.hi[h] = iv.hi15;
                 cp.pad[h] = 0;
                 if (cl == 0) {
                     LineShX ls;
@@ -1295,34 +1295,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt_mc(StepArgs a) {
 // pairs, each pair one packed FP32x2 operation per step of the region-I
 // rational (u = X^2 k^2 + Cy, u^2 + D2, Pc (u + 1), accumulate), so a
 // region-I pair costs two FP32 operations and one reciprocal per condition
-// and about three issue slots in all.  Near a core, step one's region
-// intervals decide: W4 region II is evaluated in place, regions III and IV
-// are queued per warp and evaluated 32 at a time.
+// and about three issue slots in all.  The pairs inside a line's region
+// interval (|x| + y < 15, from step one) are left to k_core_mcx.
 // ---------------------------------------------------------------------------
-// W4 region II (w4_region2_re) for two conditions at once, packed FP32x2,
-// with an approximate reciprocal for the final division.
-__device__ __forceinline__ float2 w4_region2_re_x2(float2 x, float2 y) {
-    const float a = 1.410474f, b = .5641896f, c = .75f;
-    const float2 x2 = __fmul2_rn(x, x), y2 = __fmul2_rn(y, y);
-    const float2 ur = __ffma2_rn(x2, f2s(-1.0f), y2);          // y^2 - x^2
-    const float2 nui = __fmul2_rn(__fmul2_rn(x, y), f2s(2.0f));  // -ui = 2 x y
-    const float2 nr = __ffma2_rn(ur, f2s(b), f2s(a));
-    const float2 dr = __ffma2_rn(__fmul2_rn(nui, f2s(-1.0f)), nui,
-                                 __ffma2_rn(ur, __fadd2_rn(ur, f2s(3.0f)), f2s(c)));
-    const float2 e = __ffma2_rn(ur, f2s(2.0f), f2s(3.0f));     // 3 + 2 ur
-    const float2 di = __fmul2_rn(__fmul2_rn(nui, f2s(-1.0f)), e);
-    const float2 q1 = __ffma2_rn(x2, f2s(-3.0f * b), __ffma2_rn(y2, f2s(b), f2s(a)));
-    const float2 q2 = __ffma2_rn(y2, f2s(2.0f * b), nr);
-    const float2 q3 = __fmul2_rn(__fmul2_rn(x2, f2s(2.0f)), e);
-    const float2 br = __ffma2_rn(q1, dr, __fmul2_rn(q3, q2));
-    const float2 den = __ffma2_rn(dr, dr, __fmul2_rn(di, di));
-    const float2 num = __fmul2_rn(y, br);
-    return f2(num.x * rcp_approx_f32(den.x), num.y * rcp_approx_f32(den.y));
-}
-
 template <int C, int WARPS>
 constexpr int voigt_mcx_min_blocks() {
-    return C <= 2 ? 24 / WARPS : 16 / WARPS;
+    return C <= 2 ? 24 / WARPS : (C == 4 ? 20 / WARPS : 16 / WARPS);
 }
 
 template <int C, int WARPS>
@@ -1330,32 +1308,12 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
     k_steptwo_voigt_mcx(StepArgs a) {
     static_assert(C % 2 == 0, "conditions come in pairs");
     constexpr int NP = C / 2;
-    using Q = WarpCoreQueue<C, true>;  // one row per condition
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     LineShX* lsb = reinterpret_cast<LineShX*>(smem_raw) + warp * 64;
     CondPairX* cpb = reinterpret_cast<CondPairX*>(smem_raw + size_t(WARPS) * 64 * sizeof(LineShX)) +
                      warp * 64 * NP;
-    Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 64 * (sizeof(LineShX) + NP * sizeof(CondPairX)))[warp];
-    const unsigned lt_mask = (1u << lane) - 1u;
-
-#pragma unroll
-    for (int c = 0; c < C; ++c) cq.corr[c][lane] = 0.0f;
-    int qn = 0;
-    // Queues this lane's pair when `need` (x, y, pref of condition c).
-    auto push = [&](bool need, float x, float y, float pref, int c) {
-        const unsigned b = __ballot_sync(0xffffffffu, need);
-        if (need) {
-            CoreEntry<float> e;
-            e.x = x;
-            e.y = y;
-            e.pref = pref;
-            e.dest = lane | (c << 5);
-            cq.q[qn + __popc(b & lt_mask)] = e;
-        }
-        qn += __popc(b);
-    };
 
     for (;;) {
         int item = 0;
@@ -1410,10 +1368,10 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         // lines whose u may overflow.
         auto region1 = [&](auto guard, float X2, const CondPairX& r, int p, bool keep0, bool keep1) {
             const float4 f0 = *reinterpret_cast<const float4*>(&r.Cy[0]);
-            const float4 f1 = *reinterpret_cast<const float4*>(&r.Pc[0]);
+            const float2 pc = *reinterpret_cast<const float2*>(&r.Pc[0]);
             const float2 u = __ffma2_rn(f2(X2, X2), k2[p], f2(f0.x, f0.y));
             const float2 den = __ffma2_rn(u, u, f2(f0.z, f0.w));
-            const float2 num = __ffma2_rn(u, f2(f1.x, f1.y), f2(f1.x, f1.y));
+            const float2 num = __ffma2_rn(u, pc, pc);
             const float2 rr = f2(keep0 ? rcp_approx_f32(den.x) : 0.0f, keep1 ? rcp_approx_f32(den.y) : 0.0f);
             if constexpr (decltype(guard)::value) {
                 acc[p].x += keep0 ? num.x * rr.x : 0.0f;
@@ -1476,10 +1434,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, in, in);
                 }
             };
-            // Core candidates.  Per condition whose region interval reaches
-            // the row: pairs with |x| + y < 15 drop out of region I; region
-            // II is evaluated in place for both conditions of the pair at
-            // once, regions III and IV are queued.
+            // Core candidates: region I outside each condition's interval.
             auto cand_run = [&](int x, int y) {
                 for (int t = x; t < y; ++t) {
                     const LineShX s = SL[t];
@@ -1488,53 +1443,17 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     const float X = s.whole ? float((s.nu - fj) / s.nu) : fmaf(s.m - jf, s.dfn, s.rn);
                     const float X2 = X * X;
                     const float aX = fabsf(X);
-                    const int mline = int(s.m);
-                    const int rel = jj - mline;
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
                         const CondPairX& r = SC[t * NP + p];
-                        bool keep[2], r2[2], deep[2], queue[2];
-                        float ax[2];
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int c15 = r.c15[h];
-                            keep[h] = in;
-                            r2[h] = deep[h] = queue[h] = false;
-                            ax[h] = aX * kx[2 * p + h];
-                            if (c15 == kCoreWhole) {
-                                const float sx = ax[h] + r.y[h];
-                                const bool i15 = sx < 15.0f, i55 = sx < 5.5f;
-                                // beyond x ~ 1e9 region I is taken as 0
-                                keep[h] = in && !i15 && ax[h] < 1.0e9f;
-                                r2[h] = in && i15 && !i55;
-                                deep[h] = in && i55;
-                                queue[h] = true;
-                            } else if (c15 != kCoreNone) {
-                                const int lo = int(short(c15 & 0xffff)), hi = c15 >> 16;
-                                if (lo <= tl - mline && hi >= t0 - mline) {
-                                    const int c55 = r.c55[h];
-                                    const int lo5 = int(short(c55 & 0xffff)), hi5 = c55 >> 16;
-                                    const bool i15 = rel >= lo && rel <= hi;
-                                    const bool i55 = rel >= lo5 && rel <= hi5;  // kCoreNone: empty
-                                    keep[h] = in && !i15;
-                                    r2[h] = in && i15 && !i55;
-                                    deep[h] = in && i55;
-                                    queue[h] = lo5 <= tl - mline && hi5 >= t0 - mline;
-                                }
-                            }
-                        }
-                        region1(guarded, X2, r, p, keep[0], keep[1]);
-                        if (__any_sync(0xffffffffu, r2[0] || r2[1])) {
-                            const float2 w = w4_region2_re_x2(f2(ax[0], ax[1]), f2(r.y[0], r.y[1]));
-                            acc[p].x += r2[0] ? r.pref[0] * w.x : 0.0f;
-                            acc[p].y += r2[1] ? r.pref[1] * w.y : 0.0f;
-                        }
+                        bool keep[2];
 #pragma unroll
                         for (int h = 0; h < 2; ++h)
-                            if (queue[h]) push(deep[h], ax[h], r.y[h], r.pref[h], 2 * p + h);
+                            // beyond x ~ 1e9 (lines far off the FP32 offset
+                            // range) region I is taken as 0
+                            keep[h] = in && !(jj >= r.lo[h] && jj <= r.hi[h]) && aX * kx[2 * p + h] < 1.0e9f;
+                        region1(guarded, X2, r, p, keep[0], keep[1]);
                     }
-                    __syncwarp();
-                    while (qn >= 32) qn = core_queue_flush<C, true>(cq, qn, 32, lane);
                 }
             };
             fast_run(a1, min(d1, b1));
@@ -1544,9 +1463,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             masked_run(d1, min(e1, b1));
             masked_run(max(d1, c1), e1);
             cand_run(b1, c1);
-            // Pending core pairs, then the compensated (Kahan) fold of this
-            // group's FP32 partials.
-            while (qn > 0) qn = core_queue_flush<C, true>(cq, qn, qn < 32 ? qn : 32, lane);
+            // compensated (Kahan) fold of this group's FP32 partials
             auto kahan = [](float part, float& sm, float& cm) {
                 const float yk = part - cm;
                 const float tk = sm + yk;
@@ -1555,10 +1472,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             };
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
-                kahan(acc[p].x + cq.corr[2 * p][lane], sum[p].x, cmp[p].x);
-                kahan(acc[p].y + cq.corr[2 * p + 1][lane], sum[p].y, cmp[p].y);
-                cq.corr[2 * p][lane] = 0.0f;
-                cq.corr[2 * p + 1][lane] = 0.0f;
+                kahan(acc[p].x, sum[p].x, cmp[p].x);
+                kahan(acc[p].y, sum[p].y, cmp[p].y);
                 acc[p] = f2(0.0f, 0.0f);
             }
             __syncwarp();
@@ -1571,6 +1486,68 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             }
         }
     }
+}
+
+// Core pass of the mixed multi-condition layout.  A warp takes a (condition,
+// row of 32 grid points); the lines whose region interval may reach the row
+// form one run (the nearest grid index mi[] is ascending; the condition's
+// widest interval bounds the reach), taken 32 at a time: each lane evaluates
+// W4 regions II-IV (region III-IV interval from step one, region III or IV
+// by Humlicek's test on the FP32 x, y) at the row's points inside its line's
+// interval and writes them to a per-warp table, then each lane adds its
+// point's column in line order.  Sums are FP32 per batch of 32 lines and FP64
+// across batches, in a fixed order.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
+    __shared__ float tab[WARPS][32][33];  // [line of the batch][point], padded
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int c = int(blockIdx.y);
+    const int t0 = a.G.start + (int(blockIdx.x) * WARPS + warp) * 32;
+    const int end = a.G.start + a.G.points;
+    if (t0 >= end) return;
+    const int t1 = t0 + 32 < end ? t0 + 32 : end;
+    const int tl = t1 - 1;
+    const int K = a.kc[c];
+    const long E = warp_lower_bound(0, a.n, lane, [&](long i) { return a.mi[i] >= t0 - K; });
+    const long F = warp_lower_bound(E, a.n, lane, [&](long i) { return a.mi[i] > tl + K; });
+    const CoreIv* civ = a.civ + size_t(c) * size_t(a.n);
+    const float2* cyp = a.cyp + size_t(c) * size_t(a.n);
+    const LineShX* lsh = a.lsh + size_t(c / a.group) * size_t(a.n);
+    const float k = a.kx[c];
+    float (*T)[33] = tab[warp];
+    double acc = 0.0;
+    for (long b = E; b < F; b += 32) {
+#pragma unroll
+        for (int q = 0; q < 32; ++q) T[lane][q] = 0.0f;
+        const long i = b + lane;
+        if (i < F) {
+            const CoreIv iv = civ[i];
+            const int jlo = max(iv.lo15, t0), jhi = min(iv.hi15, tl);
+            if (jlo <= jhi) {
+                const LineShX s = lsh[i];
+                const float2 yp = cyp[i];
+                for (int j = jlo; j <= jhi; ++j) {
+                    const float X = s.whole ? float((s.nu - a.freq[j]) / s.nu) : fmaf(s.m - float(j), s.dfn, s.rn);
+                    const float ax = fabsf(X) * k, y = yp.x;
+                    float w;
+                    if (j >= iv.lo55 && j <= iv.hi55)
+                        w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y) : w4_region4_re_f32(ax, y);
+                    else
+                        w = w4_region2_re<float>(ax, y);
+                    T[lane][j - t0] = yp.y * w;
+                }
+            }
+        }
+        __syncwarp();
+        const long nb = F - b < 32 ? F - b : 32;
+        float part = 0.0f;
+        for (int t = 0; t < int(nb); ++t) part += T[t][lane];
+        acc += double(part);
+        __syncwarp();
+    }
+    const int jj = t0 + lane;
+    if (jj < t1) a.out[size_t(a.row[c]) * a.out_stride + size_t(jj)] += acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -1715,8 +1692,7 @@ cudaError_t run_voigt_mc(int blocks, const StepArgs& a, cudaStream_t st, int* oc
 
 template <int C, int WARPS>
 cudaError_t run_voigt_mcx(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
-    const size_t smem = size_t(WARPS) * (64 * (sizeof(LineShX) + (C / 2) * sizeof(CondPairX)) +
-                                         sizeof(WarpCoreQueue<C, true>));
+    const size_t smem = size_t(WARPS) * 64 * (sizeof(LineShX) + (C / 2) * sizeof(CondPairX));
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(k_steptwo_voigt_mcx<C, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)) != cudaSuccess)
@@ -1867,6 +1843,14 @@ int steptwo_blocks_per_sm(int kind, int conv, bool mixed, int P, int warps) {
     return occ;
 }
 
+cudaError_t launch_core_mcx(const CoreArgs& a, int ncond, cudaStream_t stream) {
+    if (a.n <= 0 || a.G.points <= 0 || ncond <= 0) return cudaSuccess;
+    constexpr int W = 4;
+    const int rows = (a.G.points + 31) / 32;
+    k_core_mcx<W><<<dim3(unsigned((rows + W - 1) / W), unsigned(ncond)), W * 32, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_steptwo_mc(bool mixed, int C, int warps, int blocks, const StepArgs& a,
                               cudaStream_t stream) {
     if (blocks <= 0 || a.n_items <= 0) return cudaSuccess;
@@ -1898,7 +1882,10 @@ ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_
     p.off_kc = al(p.off_mi + sizeof(int) * n);
     p.off_lsh = al(p.off_kc + sizeof(int) * size_t(kMaxCond));
     const size_t lsh = mixed ? sizeof(LineShX) : sizeof(LineSh64);
-    p.need = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
+    p.off_civ = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
+    const bool core = mixed && group > 0;
+    p.off_cyp = al(p.off_civ + (core ? sizeof(CoreIv) * n * size_t(ncond) : 0));
+    p.need = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
     return p;
 }
 

@@ -439,13 +439,14 @@ def test_graph_replay_matches_execute(engine, cuda):
             engine.sync()
             assert torch.equal(replay, direct)
             assert engine.last_stats()[1] > 0
-        # grid check, step one, step two (+ the split reduction)
-        assert g.kernel_count() in (3, 4)
+        # grid check, step one, step two, the core pass (+ the split reduction)
+        assert g.kernel_count() in (4, 5)
     finally:
         g.close()
     one = capi.make_options(capi.VOIGT, grid.dfreq, 17.03, precision=capi.MIXED, line_splits=1)
     two = capi.make_options(capi.VOIGT, grid.dfreq, 17.03, precision=capi.MIXED, line_splits=2)
-    for o, kernels in ((one, 3), (two, 4)):
+    f64 = capi.make_options(capi.VOIGT, grid.dfreq, 17.03, line_splits=1, conditions_per_warp=1)
+    for o, kernels in ((one, 4), (two, 5), (f64, 3)):
         g = engine.capture(o, conds, capi.make_lines(d), capi.make_grid(dfr), replay.data_ptr(), len(fr),
                            zero_out=True)
         try:
