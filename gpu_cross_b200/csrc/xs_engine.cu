@@ -775,7 +775,7 @@ int xs_engine_autotune(xs_engine* e, const xs_options* opt, const xs_condition* 
             cands.push_back({P, W, kind == XS_VOIGT ? 1 : 0});
         }
         if (kind == XS_VOIGT && ncond > 1)
-            for (int C : {2, 4})
+            for (int C : {2, 4, 8})
                 if (ncond % C == 0 && ncond <= kMaxCond) cands.push_back({1, W, C});
     }
     long n = long(lines->count);
