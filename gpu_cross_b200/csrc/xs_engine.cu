@@ -429,7 +429,12 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     const ScratchPlan plan = plan_scratch(kind, mixed, size_t(n), group, 0, CG);
     int occ = CG ? steptwo_mc_blocks_per_sm(mixed, CG, W)
                  : steptwo_blocks_per_sm(kind, opt->convention, mixed, P, W);
-    if (occ < 1) occ = 1;
+    if (occ < 1) {
+        // e.g. 8 FP64 conditions per warp with 8 warps: more shared memory
+        // than a block can have
+        cudaGetLastError();
+        return fail(XS_ERR_INVALID, "this launch shape cannot run on the device (shared memory)");
+    }
 
     // Line splits.  Work items are taken dynamically, but an item is a whole
     // tile over all its lines: with fewer items than resident warps (short
@@ -555,7 +560,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.cyp = reinterpret_cast<float2*>(base + plan.off_cyp);
 
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, ev_flags);
-        err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(kMaxCond), st);
+        err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(2 * kMaxCond), st);
         if (err != cudaSuccess) return cuda_fail(err, "core-width reset");
         err = launch_prep(kind, opt->convention, mixed, pa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step one launch");

@@ -177,7 +177,9 @@ struct PrepArgs {
     int* wlo;           // windows, condition-major
     int* whi;
     int* mi;            // nearest grid index of each line (condition-free)
-    int* kc;            // per condition: max core half-width in grid points
+    int* kc;            // per condition: max core half-width in grid points;
+                        // kc + kMaxCond: the core pass's reach (mixed
+                        // multi-condition layout)
     unsigned* err;
     double half_width;  // Gaussian
     double x0;          // Doppler half bin: dfreq * 0.5

@@ -127,10 +127,13 @@ __global__ void k_grid_check(GridDev g, unsigned* err) {
 // Step one.
 // ---------------------------------------------------------------------------
 // Returns the line's core half-width in grid points (Voigt; 0 otherwise).
+// `reach` (mixed multi-condition layout): the largest distance, in grid
+// points, from the line's nearest grid index to its region interval.
 // `pair`: the mixed-precision multi-condition layout fills its condition's
 // half of a CondPairX there (k_prep_pairs stores the whole record).
 template <int KIND, int CONV, bool MIXED>
-__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondPairX* pair = nullptr) {
+__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondPairX* pair = nullptr,
+                                         int* reach = nullptr) {
     const CondDev& C = a.cond[c];
     const double* F = a.G.freq;
     const double f0 = F[0];
@@ -281,15 +284,14 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
                 CoreIv iv;
                 interval(15.0, iv.lo15, iv.hi15);
                 interval(5.5, iv.lo55, iv.hi55);
-                if (whole) {
-                    kcl = 30000000;  // every tile takes the line as a core candidate
-                } else {
-                    kcl = 0;
-                    if (iv.lo15 <= iv.hi15) {
-                        const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
-                        kcl = w < 3.0e7 ? int(w) : 30000000;
-                    }
+                int rch = 0;
+                if (iv.lo15 <= iv.hi15) {
+                    const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
+                    rch = w < 3.0e7 ? int(w) : 30000000;
                 }
+                if (reach) *reach = rch;
+                // a whole line is a core candidate of every tile
+                kcl = whole ? 30000000 : rch;
                 const size_t ci2 = size_t(c) * size_t(a.L.n) + size_t(i);
                 a.civ[ci2] = iv;
                 a.cyp[ci2] = make_float2(float(y), float(pref));
@@ -411,11 +413,11 @@ template <int CONV>
 __global__ void __launch_bounds__(256) k_prep_pairs(PrepArgs a) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     const int c0 = 2 * int(blockIdx.y);
-    int k0 = 0, k1 = 0;
+    int k0 = 0, k1 = 0, r0 = 0, r1 = 0;
     if (i < a.L.n) {
         CondPairX cp;
-        k0 = prep_line<kVoigt, CONV, true>(a, i, c0, &cp);
-        k1 = prep_line<kVoigt, CONV, true>(a, i, c0 + 1, &cp);
+        k0 = prep_line<kVoigt, CONV, true>(a, i, c0, &cp, &r0);
+        k1 = prep_line<kVoigt, CONV, true>(a, i, c0 + 1, &cp, &r1);
         const int C = a.group;
         const int cg = c0 / C;
         const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(i);
@@ -424,18 +426,25 @@ __global__ void __launch_bounds__(256) k_prep_pairs(PrepArgs a) {
 #pragma unroll
         for (int q = 0; q < int(sizeof(CondPairX) / 16); ++q) dst[q] = src[q];
     }
-    __shared__ int smax[2][8];
+    // block maxima of the core-candidate widths (kc) and of the core pass's
+    // reach (kc + kMaxCond), one atomic each per block
+    __shared__ int smax[4][8];
     k0 = __reduce_max_sync(0xffffffffu, k0);
     k1 = __reduce_max_sync(0xffffffffu, k1);
+    r0 = __reduce_max_sync(0xffffffffu, r0);
+    r1 = __reduce_max_sync(0xffffffffu, r1);
     if ((threadIdx.x & 31) == 0) {
         smax[0][threadIdx.x >> 5] = k0;
         smax[1][threadIdx.x >> 5] = k1;
+        smax[2][threadIdx.x >> 5] = r0;
+        smax[3][threadIdx.x >> 5] = r1;
     }
     __syncthreads();
-    if (threadIdx.x < 2) {
+    if (threadIdx.x < 4) {
         int m = 0;
         for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[threadIdx.x][w] > m ? smax[threadIdx.x][w] : m;
-        if (m > 0) atomicMax(a.kc + c0 + int(threadIdx.x), m);
+        const int slot = (threadIdx.x >= 2 ? kMaxCond : 0) + c0 + int(threadIdx.x & 1);
+        if (m > 0) atomicMax(a.kc + slot, m);
     }
 }
 
@@ -1508,7 +1517,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     if (t0 >= end) return;
     const int t1 = t0 + 32 < end ? t0 + 32 : end;
     const int tl = t1 - 1;
-    const int K = a.kc[c];
+    const int K = a.kc[kMaxCond + c];  // the condition's core-pass reach
     const long E = warp_lower_bound(0, a.n, lane, [&](long i) { return a.mi[i] >= t0 - K; });
     const long F = warp_lower_bound(E, a.n, lane, [&](long i) { return a.mi[i] > tl + K; });
     const CoreIv* civ = a.civ + size_t(c) * size_t(a.n);
@@ -1880,7 +1889,7 @@ ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_
     p.off_whi = al(p.off_wlo + sizeof(int) * n * nwin);
     p.off_mi = al(p.off_whi + sizeof(int) * n * nwin);
     p.off_kc = al(p.off_mi + sizeof(int) * n);
-    p.off_lsh = al(p.off_kc + sizeof(int) * size_t(kMaxCond));
+    p.off_lsh = al(p.off_kc + sizeof(int) * size_t(2 * kMaxCond));
     const size_t lsh = mixed ? sizeof(LineShX) : sizeof(LineSh64);
     p.off_civ = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
     const bool core = mixed && group > 0;
