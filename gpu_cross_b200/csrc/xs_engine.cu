@@ -607,11 +607,9 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
                 : launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step two launch");
         if (blocks > 0 && sa.n_items > 0) ++launched;
-        err = launch_reduce_splits(sa, nc, st);
-        if (err != cudaSuccess) return cuda_fail(err, "split reduction launch");
-        if (S > 1) ++launched;
         if (CG && mixed) {
-            // the pairs inside the lines' region intervals (W4 regions II-IV)
+            // the pairs inside the lines' region intervals (W4 regions II-IV),
+            // into the split parts before they are added up
             CoreArgs ca;
             std::memset(&ca, 0, sizeof(ca));
             ca.civ = pa.civ;
@@ -625,6 +623,9 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
             ca.G = G;
             ca.out = out;
             ca.out_stride = out_stride;
+            ca.splits = S;
+            ca.part = sa.part;
+            ca.part_stride = sa.part_stride;
             for (int c = 0; c < nc; ++c) {
                 ca.kx[c] = sa.kx[c];
                 ca.row[c] = sa.row[c];
@@ -633,6 +634,9 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
             if (err != cudaSuccess) return cuda_fail(err, "core pass launch");
             ++launched;
         }
+        err = launch_reduce_splits(sa, nc, st);
+        if (err != cudaSuccess) return cuda_fail(err, "split reduction launch");
+        if (S > 1) ++launched;
         if (timing && c0 + nc >= ncond) {
             cudaEventRecordWithFlags(e->ev[2], st, ev_flags);
             e->timed = true;

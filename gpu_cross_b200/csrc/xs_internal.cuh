@@ -260,6 +260,13 @@ struct CoreArgs {
     GridDev G;
     double* out;
     size_t out_stride;
+    // Line splits as in StepArgs: with splits > 1 the warp of split s takes
+    // the 32-line batches s, s + splits, ... of a row's candidate lines and
+    // adds its sums to the step-two parts, which k_reduce_splits then adds in
+    // order; with one split it adds to out.
+    int splits;
+    double* part;
+    size_t part_stride;
     float kx[kMaxCond];  // 1 / dpw
     int row[kMaxCond];
 };

@@ -1505,7 +1505,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
 // by Humlicek's test on the FP32 x, y) at the row's points inside its line's
 // interval and writes them to a per-warp table, then each lane adds its
 // point's column in line order.  Sums are FP32 per batch of 32 lines and FP64
-// across batches, in a fixed order.
+// across batches, in a fixed order.  With line splits (blockIdx.z = split) a
+// row's batches are shared out as in step two and the sums go to the parts.
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     __shared__ float tab[WARPS][32][33];  // [line of the batch][point], padded
@@ -1525,8 +1526,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     const LineShX* lsh = a.lsh + size_t(c / a.group) * size_t(a.n);
     const float k = a.kx[c];
     float (*T)[33] = tab[warp];
+    const int split = int(blockIdx.z), S = a.splits;
     double acc = 0.0;
-    for (long b = E; b < F; b += 32) {
+    for (long b = E + 32L * split; b < F; b += 32L * S) {
 #pragma unroll
         for (int q = 0; q < 32; ++q) T[lane][q] = 0.0f;
         const long i = b + lane;
@@ -1556,7 +1558,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
         __syncwarp();
     }
     const int jj = t0 + lane;
-    if (jj < t1) a.out[size_t(a.row[c]) * a.out_stride + size_t(jj)] += acc;
+    if (jj < t1) {
+        if (S <= 1)
+            a.out[size_t(a.row[c]) * a.out_stride + size_t(jj)] += acc;
+        else
+            a.part[(size_t(c) * S + split) * a.part_stride + size_t(jj - a.G.start)] += acc;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1856,7 +1863,8 @@ cudaError_t launch_core_mcx(const CoreArgs& a, int ncond, cudaStream_t stream) {
     if (a.n <= 0 || a.G.points <= 0 || ncond <= 0) return cudaSuccess;
     constexpr int W = 4;
     const int rows = (a.G.points + 31) / 32;
-    k_core_mcx<W><<<dim3(unsigned((rows + W - 1) / W), unsigned(ncond)), W * 32, 0, stream>>>(a);
+    const unsigned S = unsigned(a.splits > 1 ? a.splits : 1);
+    k_core_mcx<W><<<dim3(unsigned((rows + W - 1) / W), unsigned(ncond), S), W * 32, 0, stream>>>(a);
     return cudaGetLastError();
 }
 
