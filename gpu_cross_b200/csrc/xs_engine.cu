@@ -590,14 +590,14 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         sa.x0g = pa.x0g;
         err = cudaMemsetAsync(sa.counter, 0, sizeof(unsigned), st);
         if (err != cudaSuccess) return cuda_fail(err, "counter reset");
+        for (int c = 0; c < nc; ++c) {
+            const double k = 1.0 / pa.cond[c].dpw;
+            sa.kx[c] = float(k);
+            sa.kx2[c] = float(k * k);
+        }
         if (CG) {
             sa.lsh = pa.lsh;
             sa.group = CG;
-            for (int c = 0; c < nc; ++c) {
-                const double k = 1.0 / pa.cond[c].dpw;
-                sa.kx[c] = float(k);
-                sa.kx2[c] = float(k * k);
-            }
             sa.tiles_per_cond = (grid->points + 31) / 32;
             sa.n_items = sa.tiles_per_cond * (nc / CG) * S;
         }
@@ -631,6 +631,12 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
                 ca.row[c] = sa.row[c];
             }
             err = launch_core_mcx(ca, nc, st);
+            if (err != cudaSuccess) return cuda_fail(err, "core pass launch");
+            ++launched;
+        } else if (mixed) {
+            // single-condition layout: the pairs inside the records' region
+            // intervals (W4 regions II-IV), into the split parts if any
+            err = launch_core_v32(sa, nc, st);
             if (err != cudaSuccess) return cuda_fail(err, "core pass launch");
             ++launched;
         }

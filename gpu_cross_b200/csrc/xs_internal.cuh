@@ -77,12 +77,17 @@ static_assert(sizeof(RecV64) == 80, "RecV64 layout");
 // Mixed-precision record (FP32).  The offset of grid point j from the line
 // centre is (m - j) * df + r in cm-1, with m the nearest grid index and
 // |r| <= df/2 computed in FP64; stored scaled by g: x = (m - j) * dfa + ra.
-// The first two 16-byte chunks are all the fast path reads.
+// The first two 16-byte chunks are all the fast path reads.  [clo, chi]:
+// the grid indices of the line's window where |x| + y < 15 (W4 regions
+// II-IV, left to the core pass; empty: clo > chi), [lo55, hi55] those where
+// |x| + y < 5.5.  A negative dfa marks a line whose x comes from its FP64
+// centre (|m| >= 1.6e7, or offsets beyond the FP32 range over the window).
 struct __align__(16) RecV32 {
     float m, ra, dfa, Cy;
     float D2, Pc, pref, y;
     float lo, hi, clo, chi;
-    float pad0, pad1, pad2, pad3;
+    float lo55, hi55;
+    double nu;
 };
 static_assert(sizeof(RecV32) == 64, "RecV32 layout");
 
@@ -271,6 +276,9 @@ struct CoreArgs {
     int row[kMaxCond];
 };
 cudaError_t launch_core_mcx(const CoreArgs& a, int ncond, cudaStream_t stream);
+// The same for the single-condition mixed layout (RecV32 records; a.kx set;
+// with line splits it adds to a.part).
+cudaError_t launch_core_v32(const StepArgs& a, int ncond, cudaStream_t stream);
 
 // Multi-condition step two (Voigt): C conditions per warp, 32 points per warp.
 cudaError_t launch_steptwo_mc(bool mixed, int C, int warps, int blocks, const StepArgs& a,

@@ -127,8 +127,29 @@ __global__ void k_grid_check(GridDev g, unsigned* err) {
 // Step one.
 // ---------------------------------------------------------------------------
 // Returns the line's core half-width in grid points (Voigt; 0 otherwise).
-// `reach` (mixed multi-condition layout): the largest distance, in grid
-// points, from the line's nearest grid index to its region interval.
+// Grid indices [jlo, jhi] of the window [lo, hi) where |x| + y < lim, with
+// x = (nu - f_j) g in FP64 on the analytic grid f_j = f0 + j df: the region
+// choice of the FP64 path (up to the grid's last-bit rounding), so that no
+// pair changes region with the FP32 rounding of x.  Empty: jlo > jhi.
+__device__ void region_interval(double nu, double g, double y, double lim, int lo, int hi, double f0,
+                                double df, int& jlo, int& jhi) {
+    jlo = 1;
+    jhi = 0;
+    if (!(y < lim) || lo >= hi) return;
+    auto fa = [&](int j) { return fma(double(j), df, f0); };
+    auto inside = [&](int j) { return !(fabs((nu - fa(j)) * g) + y >= lim); };
+    const double hw = (lim - y) / g;
+    const int jl = find_first(lo, hi, ceil((nu - hw - f0) / df), [&](int j) { return fa(j) > nu || inside(j); });
+    const int jh = find_first(lo, hi, floor((nu + hw - f0) / df) + 1.0,
+                              [&](int j) { return fa(j) > nu && !inside(j); });
+    if (jl < jh) {
+        jlo = jl;
+        jhi = jh - 1;
+    }
+}
+
+// `reach` (mixed Voigt): the largest distance, in grid points, from the
+// line's nearest grid index to its region interval (the core pass's reach).
 // `pair`: the mixed-precision multi-condition layout fills its condition's
 // half of a CondPairX there (k_prep_pairs stores the whole record).
 template <int KIND, int CONV, bool MIXED>
@@ -265,25 +286,9 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
                 // flips with the FP32 rounding of x.  Step two leaves the
                 // pairs of [lo15, hi15] to the core pass.
                 const bool far_m = !(fabs(m) < 16000000.0);
-                auto interval = [&](double lim, int& jlo, int& jhi) {
-                    jlo = 1;
-                    jhi = 0;
-                    if (!(y < lim) || lo >= hi) return;
-                    auto fa = [&](int j) { return fma(double(j), df, f0); };
-                    auto inside = [&](int j) { return !(fabs((nu_p - fa(j)) * g) + y >= lim); };
-                    const double hw = (lim - y) / g;
-                    const int jl = find_first(lo, hi, ceil((nu_p - hw - f0) / df),
-                                              [&](int j) { return fa(j) > nu_p || inside(j); });
-                    const int jh = find_first(lo, hi, floor((nu_p + hw - f0) / df) + 1.0,
-                                              [&](int j) { return fa(j) > nu_p && !inside(j); });
-                    if (jl < jh) {
-                        jlo = jl;
-                        jhi = jh - 1;
-                    }
-                };
                 CoreIv iv;
-                interval(15.0, iv.lo15, iv.hi15);
-                interval(5.5, iv.lo55, iv.hi55);
+                region_interval(nu_p, g, y, 15.0, lo, hi, f0, df, iv.lo15, iv.hi15);
+                region_interval(nu_p, g, y, 5.5, lo, hi, f0, df, iv.lo55, iv.hi55);
                 int rch = 0;
                 if (iv.lo15 <= iv.hi15) {
                     const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
@@ -344,7 +349,7 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
             RecV32 rr;
             rr.m = float(fabs(m) < 16000000.0 ? m : 0.0);
             rr.ra = float(((nu_p - f0) - m * df) * g);
-            rr.dfa = float(df * g);
+            rr.dfa = float(whole ? -df * g : df * g);  // negative: x from the FP64 centre
             rr.Cy = float(Cy);
             rr.D2 = float(D2);
             rr.Pc = float(Pc);
@@ -352,9 +357,22 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
             rr.y = float(y);
             rr.lo = float(lo);
             rr.hi = float(hi);
-            rr.clo = float(clo_d);
-            rr.chi = float(chi_d);
-            rr.pad0 = rr.pad1 = rr.pad2 = rr.pad3 = 0.0f;
+            // exact intervals: step two leaves [clo, chi] to the core pass
+            int j15, k15, j55, k55;
+            region_interval(nu_p, g, y, 15.0, lo, hi, f0, df, j15, k15);
+            region_interval(nu_p, g, y, 5.5, lo, hi, f0, df, j55, k55);
+            int rch = 0;
+            if (j15 <= k15) {
+                const double w = fmax(m - double(j15), double(k15) - m);
+                rch = w < 3.0e7 ? int(w) : 30000000;
+            }
+            if (reach) *reach = rch;
+            kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
+            rr.clo = float(j15);
+            rr.chi = float(k15);
+            rr.lo55 = float(j55);
+            rr.hi55 = float(k55);
+            rr.nu = nu_p;
             reinterpret_cast<RecV32*>(a.rec)[ci] = rr;
         } else {
             RecV64 rr;
@@ -452,18 +470,23 @@ template <int KIND, int CONV, bool MIXED>
 __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
-    int kcl = 0;
-    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c);
+    int kcl = 0, rch = 0;
+    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, nullptr, &rch);
     if (KIND == kVoigt) {
-        // Block maximum of the core widths, one atomic per block.
-        __shared__ int smax[8];
+        // Block maxima of the core widths (kc) and, mixed, of the core pass's
+        // reach (kc + kMaxCond), one atomic each per block.
+        __shared__ int smax[2][8];
         kcl = __reduce_max_sync(0xffffffffu, kcl);
-        if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = kcl;
+        rch = __reduce_max_sync(0xffffffffu, rch);
+        if ((threadIdx.x & 31) == 0) {
+            smax[0][threadIdx.x >> 5] = kcl;
+            smax[1][threadIdx.x >> 5] = rch;
+        }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 2) {
             int m = 0;
-            for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[w] > m ? smax[w] : m;
-            if (m > 0) atomicMax(a.kc + c, m);
+            for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[threadIdx.x][w] > m ? smax[threadIdx.x][w] : m;
+            if (m > 0) atomicMax(a.kc + (threadIdx.x ? kMaxCond : 0) + c, m);
         }
     }
 }
@@ -743,13 +766,17 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     REC* buf = reinterpret_cast<REC*>(smem_raw) + warp * 32 * kStages;
+    // the core queue (FP64 only: the mixed path leaves regions II-IV to
+    // k_core_v32 and has no queue in shared memory)
     Q& cq = reinterpret_cast<Q*>(smem_raw + size_t(WARPS) * 32 * kStages * sizeof(REC))[warp];
     const REC* recs_all = reinterpret_cast<const REC*>(a.rec);
     const double* F = a.G.freq;
     const unsigned lt_mask = (1u << lane) - 1u;
 
+    if constexpr (!MIXED) {
 #pragma unroll
-    for (int p = 0; p < P; ++p) cq.corr[p][lane] = T(0);
+        for (int p = 0; p < P; ++p) cq.corr[p][lane] = T(0);
+    }
     int qn = 0;  // entries in the queue (warp-uniform)
 
     auto push = [&](bool need, T x, T y, T pref, int p) {
@@ -839,34 +866,34 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
         // `full`: the line's window covers the whole tile.
         auto slow_line = [&](const REC& r, bool full) {
             if (MIXED) {
+                // region I except the pairs of the region interval [clo, chi]
+                // (the core pass takes those)
                 const float4* q = reinterpret_cast<const float4*>(&r);
                 const float4 v0 = q[0], v1 = q[1], v2 = q[2];
                 const float m = v0.x, ra = v0.y, dfa = v0.z, Cy = v0.w;
-                const float D2 = v1.x, Pc = v1.y, pref = v1.z, y = v1.w;
+                const float D2 = v1.x, Pc = v1.y;
                 const float lo = v2.x, hi = v2.y, clo = v2.z, chi = v2.w;
+                const bool whole = dfa < 0.0f;
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
                     const float r0 = float(t0 + 32 * p), r1 = r0 + 31.0f;
                     if (!full && (r0 >= hi || r1 < lo)) continue;
                     const bool row_in = full || (r0 >= lo && r1 < hi);
-                    const bool row_core = !(r1 < clo || r0 > chi);
-                    const float xs = fmaf(m - jf[p], dfa, ra);
+                    const bool row_core = whole || !(r1 < clo || r0 > chi);
+                    const float xs = whole ? float((r.nu - F[jj[p] < t1 ? jj[p] : tl]) / r.nu) * a.kx[w.c]
+                                           : fmaf(m - jf[p], dfa, ra);
                     const float u = fmaf(xs, xs, Cy);
-                    const float v = fmaf(u, Pc, Pc) * rcp_approx_f32(fmaf(u, u, D2));
+                    const float num = fmaf(u, Pc, Pc);
+                    const float rr = rcp_approx_f32(fmaf(u, u, D2));
                     if (row_in && !row_core) {
-                        accf[p] += v;
+                        accf[p] = fmaf(num, rr, accf[p]);
                         continue;
                     }
                     const bool in = row_in || (jf[p] >= lo && jf[p] < hi);
-                    const float ax = fabsf(xs);
-                    const float sx = ax + y;
-                    const bool band = row_core && jf[p] >= clo && jf[p] <= chi;
-                    const bool r2 = in && band && sx < 15.0f && sx >= 5.5f;
-                    const bool deep = in && band && sx < 5.5f;
-                    float add = (in && !r2 && !deep) ? v : 0.0f;
-                    if (__any_sync(0xffffffffu, r2) && r2) add = pref * w4_region2_re<float>(ax, y);
-                    accf[p] += add;
-                    if (row_core) push(deep, ax, y, pref, p);
+                    const bool core = jf[p] >= clo && jf[p] <= chi;
+                    // beyond x ~ 1e18 (whole lines only) region I is taken as 0
+                    const bool keep = in && !core && fabsf(xs) < 1.0e18f;
+                    accf[p] += keep ? num * rr : 0.0f;
                 }
             } else {
                 const double2* q = reinterpret_cast<const double2*>(&r);
@@ -909,7 +936,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
                 const float4* q = reinterpret_cast<const float4*>(&r);
                 const float4 v0 = q[0], v1 = q[1], v2 = q[2];
                 const float lo = v2.x, hi = v2.y;
-                if (!(v2.w < float(t0) || v2.z > float(tl))) {
+                // region interval reaching the tile, or a whole line
+                if (v0.z < 0.0f || !(v2.w < float(t0) || v2.z > float(tl))) {
                     slow_line(r, false);
                     return;
                 }
@@ -951,29 +979,24 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             if (MIXED) {
                 const float4* q = reinterpret_cast<const float4*>(&r);
                 const float4 v0 = q[0], v1 = q[1], v2 = q[2];
-                const float clo = v2.z, chi = v2.w, y = v1.w;
+                const float clo = v2.z, chi = v2.w;
+                const bool whole = v0.z < 0.0f;
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
                     const float r0 = float(t0 + 32 * p), r1 = r0 + 31.0f;
-                    const float xs = fmaf(v0.x - jf[p], v0.z, v0.y);
+                    const float xs = whole ? float((r.nu - F[jj[p] < t1 ? jj[p] : tl]) / r.nu) * a.kx[w.c]
+                                           : fmaf(v0.x - jf[p], v0.z, v0.y);
                     const float u = fmaf(xs, xs, v0.w);
                     const float num = fmaf(u, v1.y, v1.y);
                     const float rr = rcp_approx_f32(fmaf(u, u, v1.x));
-                    if (r1 < clo || r0 > chi) {
+                    if (!whole && (r1 < clo || r0 > chi)) {
                         accf[p] = fmaf(num, rr, accf[p]);
                         continue;
                     }
-                    // band row: region I as computed, region II in place,
-                    // regions III and IV through the queue
-                    const float ax = fabsf(xs);
-                    const float sx = ax + y;
-                    const bool band = jf[p] >= clo && jf[p] <= chi;
-                    const bool r2 = band && sx < 15.0f && sx >= 5.5f;
-                    const bool deep = band && sx < 5.5f;
-                    float add = (r2 || deep) ? 0.0f : num * rr;
-                    if (__any_sync(0xffffffffu, r2) && r2) add = v1.z * w4_region2_re<float>(ax, y);
-                    accf[p] += add;
-                    push(deep, ax, y, v1.z, p);
+                    // region I except the pairs of the region interval
+                    const bool core = jf[p] >= clo && jf[p] <= chi;
+                    const bool keep = !core && fabsf(xs) < 1.0e18f;
+                    accf[p] += keep ? num * rr : 0.0f;
                 }
             } else {
                 const double2* q = reinterpret_cast<const double2*>(&r);
@@ -1035,7 +1058,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
                 if (t >= e1) break;
                 if (t >= b1 && t < c1) core_line(R[t]);
                 else partial_line(R[t]);
-                while (qn >= 32) qn = core_queue_flush<P, MIXED>(cq, qn, 32, lane);
+                if constexpr (!MIXED)
+                    while (qn >= 32) qn = core_queue_flush<P, MIXED>(cq, qn, 32, lane);
             }
             {
                 int t = a1;
@@ -1052,13 +1076,10 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
                 if (t < d1) fast_line(R[t]);
             }
             if (MIXED) {
-                // Pending core pairs, then the compensated (Kahan) fold of
-                // this group's FP32 partials.
-                if (qn > 0) qn = core_queue_flush<P, MIXED>(cq, qn, qn, lane);
+                // compensated (Kahan) fold of this group's FP32 partials
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
-                    const float part = accf[p] + float(cq.corr[p][lane]);
-                    cq.corr[p][lane] = T(0);
+                    const float part = accf[p];
                     const float yk = part - cmpf[p];
                     const float tk = sumf[p] + yk;
                     cmpf[p] = (tk - sumf[p]) - yk;
@@ -1070,7 +1091,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
         }
         cp_async_wait<0>();
         __syncwarp();
-        if (!MIXED) {
+        if constexpr (!MIXED) {
             while (qn > 0) qn = core_queue_flush<P, MIXED>(cq, qn, qn < 32 ? qn : 32, lane);
 #pragma unroll
             for (int p = 0; p < P; ++p) {
@@ -1566,6 +1587,63 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     }
 }
 
+// Core pass of the single-condition mixed layout (RecV32): as k_core_mcx,
+// with the region intervals [clo, chi] and [lo55, hi55] of the records; a
+// line marked whole (dfa < 0) takes x from its FP64 centre.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_core_v32(StepArgs a) {
+    __shared__ float tab[WARPS][32][33];  // [line of the batch][point], padded
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int c = int(blockIdx.y);
+    const int t0 = a.G.start + (int(blockIdx.x) * WARPS + warp) * 32;
+    const int end = a.G.start + a.G.points;
+    if (t0 >= end) return;
+    const int t1 = t0 + 32 < end ? t0 + 32 : end;
+    const int tl = t1 - 1;
+    const int K = a.kc[kMaxCond + c];  // the condition's core-pass reach
+    const long E = warp_lower_bound(0, a.n, lane, [&](long i) { return a.mi[i] >= t0 - K; });
+    const long F = warp_lower_bound(E, a.n, lane, [&](long i) { return a.mi[i] > tl + K; });
+    const RecV32* recs = reinterpret_cast<const RecV32*>(a.rec) + size_t(c) * size_t(a.n);
+    const float k = a.kx[c];
+    float (*T)[33] = tab[warp];
+    const int split = int(blockIdx.z), S = a.splits;
+    double acc = 0.0;
+    for (long b = E + 32L * split; b < F; b += 32L * S) {
+#pragma unroll
+        for (int q = 0; q < 32; ++q) T[lane][q] = 0.0f;
+        const long i = b + lane;
+        if (i < F) {
+            const RecV32 r = recs[i];
+            const bool whole = r.dfa < 0.0f;
+            const int jlo = max(int(r.clo), t0), jhi = min(int(r.chi), tl);
+            for (int j = jlo; j <= jhi; ++j) {
+                const float xs = whole ? float((r.nu - a.G.freq[j]) / r.nu) * k : fmaf(r.m - float(j), r.dfa, r.ra);
+                const float ax = fabsf(xs), y = r.y;
+                float w;
+                if (float(j) >= r.lo55 && float(j) <= r.hi55)
+                    w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y) : w4_region4_re_f32(ax, y);
+                else
+                    w = w4_region2_re<float>(ax, y);
+                T[lane][j - t0] = r.pref * w;
+            }
+        }
+        __syncwarp();
+        const long nb = F - b < 32 ? F - b : 32;
+        float part = 0.0f;
+        for (int t = 0; t < int(nb); ++t) part += T[t][lane];
+        acc += double(part);
+        __syncwarp();
+    }
+    const int jj = t0 + lane;
+    if (jj < t1) {
+        if (S <= 1)
+            a.out[size_t(a.row[c]) * a.out_stride + size_t(jj)] += acc;
+        else
+            a.part[(size_t(c) * S + split) * a.part_stride + size_t(jj - a.G.start)] += acc;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Step two, Doppler and Gaussian (bin-integrated erf differences, FP64).
 // ---------------------------------------------------------------------------
@@ -1675,7 +1753,7 @@ int blocks_per_sm(K kernel, int threads, size_t smem) {
 template <int P, int WARPS, bool MIXED>
 cudaError_t run_voigt(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
     using REC = typename std::conditional<MIXED, RecV32, RecV64>::type;
-    const size_t smem = size_t(WARPS) * (32 * kStages * sizeof(REC) + sizeof(WarpCoreQueue<P, MIXED>));
+    const size_t smem = size_t(WARPS) * (32 * kStages * sizeof(REC) + (MIXED ? 0 : sizeof(WarpCoreQueue<P, MIXED>)));
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(k_steptwo_voigt<P, WARPS, MIXED>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
@@ -1857,6 +1935,15 @@ int steptwo_blocks_per_sm(int kind, int conv, bool mixed, int P, int warps) {
     if (dispatch_steptwo(kind, conv, mixed, P, warps, 0, dummy, nullptr, &occ) != cudaSuccess)
         return 0;
     return occ;
+}
+
+cudaError_t launch_core_v32(const StepArgs& a, int ncond, cudaStream_t stream) {
+    if (a.n <= 0 || a.G.points <= 0 || ncond <= 0) return cudaSuccess;
+    constexpr int W = 4;
+    const int rows = (a.G.points + 31) / 32;
+    const unsigned S = unsigned(a.splits > 1 ? a.splits : 1);
+    k_core_v32<W><<<dim3(unsigned((rows + W - 1) / W), unsigned(ncond), S), W * 32, 0, stream>>>(a);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_core_mcx(const CoreArgs& a, int ncond, cudaStream_t stream) {

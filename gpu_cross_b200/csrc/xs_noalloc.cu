@@ -4,9 +4,9 @@
 // already handed (nearly) all device memory to its own pool allocator would
 // see the allocation fail or eat into its pool, and a latency-critical loop
 // cannot afford the implicit device-wide synchronisation that cudaMalloc and
-// cudaFree may cause.  xs_execute_noalloc runs the same three kernels as
-// xs_engine_execute -- grid check, step one, persistent step two -- for one
-// condition, but takes its scratch (per-line records and windows, the error
+// cudaFree may cause.  xs_execute_noalloc runs the same kernels as
+// xs_engine_execute -- grid check, step one, persistent step two, and in
+// mixed precision the core pass -- for one condition, but takes its scratch (per-line records and windows, the error
 // word and the work counter) from one fixed array compiled into the library,
 // g_noalloc_scratch below.  It allocates nothing: no cudaMalloc, no cudaFree,
 // no engine, no events, no library routine that allocates.
@@ -182,6 +182,7 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
     sa.x0 = pa.x0;
     sa.xg = pa.xg;
     sa.x0g = pa.x0g;
+    sa.kx[0] = float(1.0 / pa.cond[0].dpw);
 
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -195,10 +196,11 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
     // work counter and the core widths must start at zero; records, windows
     // and grid indices are rewritten.
     cudaError_t e = cudaMemsetAsync(words, 0, 2 * sizeof(unsigned), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(xs::kMaxCond), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(2 * xs::kMaxCond), st);
     if (e == cudaSuccess) e = xs::launch_grid_check(G, words, st);
     if (e == cudaSuccess) e = xs::launch_prep(kind, opt->convention, mixed, pa, st);
     if (e == cudaSuccess) e = xs::launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);
+    if (e == cudaSuccess && mixed) e = xs::launch_core_v32(sa, 1, st);  // W4 regions II-IV
     // Wait for this call's kernels and report what they found.
     unsigned bits = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, words, sizeof(unsigned), cudaMemcpyDeviceToHost, st);

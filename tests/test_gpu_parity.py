@@ -209,10 +209,10 @@ def test_multi_condition_tiles_vs_oracle(engine, cuda, C):
         assert_mixed_parity(mix[k], f64[k])
 
 
-@pytest.mark.parametrize("C", [2, 4])
+@pytest.mark.parametrize("C", [1, 2, 4])
 def test_multi_condition_mixed_edges(engine, cuda, C):
-    """Mixed multi-condition tiles against FP64 where the region intervals
-    are clipped or replaced: lines centred beyond both grid ends, a grid
+    """Mixed single- and multi-condition tiles against FP64 where the region
+    intervals are clipped or replaced: lines centred beyond both grid ends, a grid
     chunk that starts inside the grid, and a grid fine enough (1e-6 cm-1)
     that the cores span more than 2^15 points and lines 20 cm-1 away lie
     more than 2^24 points from the grid's first point (pair-by-pair
