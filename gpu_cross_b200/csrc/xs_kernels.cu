@@ -703,21 +703,14 @@ struct WarpCoreQueue {
 // line: it runs once per 32 pairs and holds all of W4's regions II-IV.
 template <int P, bool MIXED>
 __device__ __noinline__ int core_queue_flush(WarpCoreQueue<P, MIXED>& cq, int qn, int k, int lane) {
+    static_assert(!MIXED, "the mixed paths evaluate their core pairs in a core pass");
     using T = typename WarpCoreQueue<P, MIXED>::T;
     T v = T(0);
     int dest = 0;
     if (lane < k) {
         const CoreEntry<T> e = cq.q[lane];
         dest = e.dest;
-        if (MIXED) {
-            // only regions III and IV are queued on the mixed path
-            const float ax = float(e.x), y = float(e.y);
-            const float w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y)
-                                                             : w4_region4_re_f32(ax, y);
-            v = T(float(e.pref) * w);
-        } else {
-            v = T(w4_re(double(e.x), double(e.y)) * double(e.pref));
-        }
+        v = T(w4_re(double(e.x), double(e.y)) * double(e.pref));
     }
     // Each push queued a run of consecutive lanes of one row, so the queue is
     // a sequence of runs (entry s + i is lane first + i).  Runs are visited in
