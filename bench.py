@@ -186,51 +186,71 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 # reference CPU (OpenMPManager compiled from the reference sources)
 # --------------------------------------------------------------------------
-def reference_cpu_sample(lines, grid, cond, common, target_s: float = 12.0, threads=None):
-    """Time the reference OpenMPManager on a nu-slice of the line list sized
-    for about target_s seconds; returns (pairs/s, threads, description)."""
+def _reference_cpu_slice(lines, cond, common, n: int):
+    """The middle n lines of the list, with gamma scaled to the condition's
+    pressure (the reference takes gamma per unit pressure as uploaded)."""
+    mid = len(lines) // 2
+    a = max(0, mid - n // 2)
+    part = lines.slice(a, a + n)
+    part.gamma = part.gamma * cond["pressure_atm"]
+    return part
+
+
+def reference_cpu_run(part, grid, cond, common, threads):
+    """One run of the reference OpenMPManager over `part` on the whole grid;
+    returns (pairs of its window, seconds)."""
     import oracle
 
-    threads = threads or os.cpu_count() or 1
     fr = grid.freq()
     c = dict(temperature=cond["temperature"], partition=cond["partition"],
              mean_mass=common["mean_mass"], pressure=1.0, ref_temp=common["ref_temp"])
-    cut = 25.0
-    mid = len(lines) // 2
+    z = np.zeros_like(fr)
+    t = time.perf_counter()
+    oracle.ref_cpu(oracle.VOIGT, fr, z, part, c, grid.dfreq, nthreads=threads)
+    dt = time.perf_counter() - t
+    return pairs_cpu_window(part.nu, fr[0], grid.dfreq, len(fr), 25.0), dt
 
-    def run(n):
-        a = max(0, mid - n // 2)
-        part = lines.slice(a, a + n)
-        part.gamma = part.gamma * cond["pressure_atm"]
-        z = np.zeros_like(fr)
-        t = time.perf_counter()
-        oracle.ref_cpu(oracle.VOIGT, fr, z, part, c, grid.dfreq, nthreads=threads)
-        dt = time.perf_counter() - t
-        return pairs_cpu_window(part.nu, fr[0], grid.dfreq, len(fr), cut), dt, part
 
+def reference_cpu_calibrate(lines, grid, cond, common, target_s: float, threads: int) -> int:
+    """Line count of a middle slice that the reference OpenMPManager takes
+    about target_s seconds for."""
     n = 20000
-    pairs, dt, part = run(n)
+    _, dt = reference_cpu_run(_reference_cpu_slice(lines, cond, common, n), grid, cond, common, threads)
     while dt < 1.0 and n < len(lines):
         n = min(len(lines), n * 4)
-        pairs, dt, part = run(n)
-    rate = pairs / dt
-    want = int(n * target_s / max(dt, 1e-3))
-    if want > n * 1.5:
-        n = min(len(lines), want)
-        pairs, dt, part = run(n)
-        rate = pairs / dt
-    desc = (f"reference OpenMPManager (g++ -O3), {threads} threads, one condition "
+        _, dt = reference_cpu_run(_reference_cpu_slice(lines, cond, common, n), grid, cond, common,
+                                  threads)
+    return int(min(len(lines), max(n, n * target_s / max(dt, 1e-3))))
+
+
+def reference_cpu_describe(part, cond, threads, pairs, dt) -> str:
+    return (f"reference OpenMPManager (g++ -O3, no -march), {threads} threads, one condition "
             f"(T={cond['temperature']:.0f} K, P={cond['pressure_atm'] / 0.986923:.3g} bar), "
             f"{len(part)} lines nu {part.nu[0]:.1f}-{part.nu[-1]:.1f} cm-1 of the 1e7-line list, "
             f"{pairs:.3e} pairs in {dt:.2f} s")
-    return rate, threads, desc
 
 
-def reference_gpu_sample(lines, grid, cond, common, n_lines: int = 400_000):
+def reference_cpu_sample(lines, grid, cond, common, target_s: float = 12.0, threads=None):
+    """Time the reference OpenMPManager on a nu-slice of the line list sized
+    for about target_s seconds; returns (pairs/s, threads, description)."""
+    threads = threads or os.cpu_count() or 1
+    n = reference_cpu_calibrate(lines, grid, cond, common, target_s, threads)
+    part = _reference_cpu_slice(lines, cond, common, n)
+    pairs, dt = reference_cpu_run(part, grid, cond, common, threads)
+    return pairs / dt, threads, reference_cpu_describe(part, cond, threads, pairs, dt)
+
+
+def reference_gpu_sample(lines, grid, cond, common, n_lines: int = 400_000, device=None):
     """Time the reference's own step-one/step-two kernels (cross_kernal.cu for
     sm_100a, oracle/_ref/libref_gpu.so) on a contiguous slice of the list for
-    one condition, chunked at 80000 grid points as BaseProfile does."""
+    one condition, chunked at 80000 grid points as BaseProfile does, and
+    compare their spectrum with the engine's plain-FP64 result for the same
+    slice and chunks (the FP64 parity tier, <= 1e-10 relative above 1e-6 of
+    the peak)."""
+    import torch
+
     import oracle
+    from gpu_cross_b200 import capi
 
     fr = grid.freq()
     mid = len(lines) // 2
@@ -241,12 +261,52 @@ def reference_gpu_sample(lines, grid, cond, common, n_lines: int = 400_000):
     span_pts = (part.nu[-1] - part.nu[0]) / grid.dfreq + 2 * 25.0 / grid.dfreq
     chunks = max(1, int(np.ceil(span_pts / 80000.0)))
     z = np.zeros_like(fr)
-    _, ms = oracle.ref_gpu(oracle.VOIGT, fr, z, part, c, grid.dfreq, chunks=chunks)
+    ref_out, ms = oracle.ref_gpu(oracle.VOIGT, fr, z, part, c, grid.dfreq, chunks=chunks)
     pairs = pairs_gpu_window(part.nu, fr, 25.0)
+
+    # the engine, FP64 and the GPU convention, over the same line chunks and
+    # grid slices (BaseProfile.cpp:55-57, as the harness applies it)
+    dev = device or torch.device("cuda", 0)
+    keys = ("nu", "energies", "aif", "gns", "gamma", "n")
+    d = {k: torch.as_tensor(np.ascontiguousarray(getattr(part, k)), device=dev) for k in keys}
+    dfr = torch.as_tensor(fr, device=dev)
+    out = torch.zeros_like(dfr)
+    eng = capi.Engine(dev.index)
+    try:
+        eng.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        opts = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.FP64,
+                                 ref_temp=common["ref_temp"])
+        cc = [capi.make_condition(cond["temperature"], cond["partition"], 1.0, 1.0, -1.0)]
+        n = len(part)
+        per = (n + chunks - 1) // chunks
+        for k in range(chunks):
+            a, b = k * per, min(n, (k + 1) * per)
+            if b <= a:
+                break
+            ib, npts = 0, len(fr)
+            if chunks > 1:
+                ib = int(max(np.round((part.nu[a] - 25.0 - fr[0]) / grid.dfreq), 0.0))
+                ie = int(min(np.round((part.nu[b - 1] + 25.0 - fr[0]) / grid.dfreq), float(len(fr))))
+                npts = ie - ib
+                if npts <= 0:
+                    continue
+            dk = {key: v[a:b] for key, v in d.items()}
+            eng.execute(opts, cc, capi.make_lines(dk), capi.make_grid(dfr, ib, npts), out.data_ptr())
+        eng.sync()
+    finally:
+        eng.close()
+    ours = out.cpu().numpy()
+    peak = np.abs(ref_out).max()
+    big = np.abs(ref_out) > 1e-6 * peak
+    rel = float(np.max(np.abs(ours[big] - ref_out[big]) / np.abs(ref_out[big]))) if big.any() else 0.0
+    small_abs = float(np.max(np.abs(ours[~big] - ref_out[~big])) / peak) if (~big).any() else 0.0
     return {"value": pairs / (ms * 1e-3), "unit": "line-evals/s", "kernel_ms": ms,
+            "fp64_vs_reference_kernel_max_rel": rel,
+            "fp64_vs_reference_kernel_max_abs_below_floor": small_abs,
             "sample": f"reference cross_kernal.cu (FP64, sm_100a) step one + step two, one condition "
                       f"(T={cond['temperature']:.0f} K), {len(part)} lines nu {part.nu[0]:.1f}-"
-                      f"{part.nu[-1]:.1f} cm-1, {chunks} chunk(s), {pairs:.3e} pairs"}
+                      f"{part.nu[-1]:.1f} cm-1, {chunks} chunk(s), {pairs:.3e} pairs; its spectrum "
+                      f"against the engine's FP64 result on the same slice and chunks"}
 
 
 # --------------------------------------------------------------------------
@@ -426,7 +486,8 @@ def run_ours(args, rank, world, dist):
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         try:
-            ref_gpu = reference_gpu_sample(lines, grid, conds[min(26, len(conds) - 1)], common)
+            ref_gpu = reference_gpu_sample(lines, grid, conds[min(26, len(conds) - 1)], common,
+                                           device=dev)
         except Exception as exc:
             ref_gpu = {"value": None, "sample": f"not run: {exc}"}
 
@@ -818,22 +879,30 @@ def run_serving(args, dev_index: int):
 
 
 def run_reference(args, rank, world):
-    """The reference's own OpenMPManager on the host cores (bounded sample per
-    step); rank 0 only."""
+    """The reference's own OpenMPManager on the host cores; rank 0 only.  A
+    step is one bounded sample of the sweep workload: one of its conditions
+    (T = 1500 K, P = 1 bar) over a middle slice of the 1e7-line list on the
+    full 7.5e4-point grid, the slice sized so that warm-up and timed steps
+    together take about --ref-seconds.  ms_per_step is the measured time of
+    that sample; value is its line-evals/s."""
     if rank != 0:
         return None
     lines, grid, conds, common = sweep_workload(args.lines, args.points, 0)
-    rates = []
-    desc, thr = "", 0
-    for _ in range(args.warmup and 1):
-        reference_cpu_sample(lines, grid, conds[min(26, len(conds) - 1)], common, target_s=min(3.0, args.cpu_seconds))
+    cond = conds[min(26, len(conds) - 1)]
+    threads = os.cpu_count() or 1
+    per_step = max(1.0, min(args.cpu_seconds, args.ref_seconds / max(1, args.steps + args.warmup)))
+    n = reference_cpu_calibrate(lines, grid, cond, common, per_step, threads)
+    part = _reference_cpu_slice(lines, cond, common, n)
+    for _ in range(args.warmup):
+        reference_cpu_run(part, grid, cond, common, threads)
+    times = []
+    pairs = 0
     for _ in range(args.steps):
-        rate, thr, desc = reference_cpu_sample(lines, grid, conds[min(26, len(conds) - 1)], common,
-                                               target_s=args.cpu_seconds)
-        rates.append(rate)
-    v = float(np.mean(rates))
-    fr = grid.freq()
-    pairs_step = pairs_gpu_window(lines.nu, fr, 25.0) * len(conds)
+        pairs, dt = reference_cpu_run(part, grid, cond, common, threads)
+        times.append(dt)
+    ms = float(np.mean(times)) * 1e3
+    v = pairs / (ms * 1e-3)
+    desc = reference_cpu_describe(part, cond, threads, pairs, ms * 1e-3)
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -842,15 +911,20 @@ def run_reference(args, rank, world):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": pairs_step / v * 1e3,
+        "ms_per_step": ms,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded)",
-        "config": {"workload": "voigt_sweep_40tp (bounded per-step sample, see cpu_baseline)",
-                   "lines": len(lines), "grid_points": len(fr), "conditions": len(conds)},
-        "cpu_baseline": {"value": v, "unit": "line-evals/s", "cores": thr, "kind": "reference",
+        "config": {"workload": (f"voigt_sweep_40tp sample: one of the 40 conditions (T "
+                                f"{cond['temperature']:.0f} K, P {cond['pressure_atm'] / 0.986923:.3g} bar), "
+                                f"{len(part)} of the 1e7 lines (middle nu slice), grid 500-8000 cm-1 at "
+                                f"0.1 (7.5e4 points), cut 25 cm-1"),
+                   "lines": len(part), "grid_points": grid.npoints, "conditions": 1,
+                   "line_evals_per_step": pairs,
+                   "full_workload": {"lines": len(lines), "conditions": len(conds)}},
+        "cpu_baseline": {"value": v, "unit": "line-evals/s", "cores": threads, "kind": "reference",
                          "sample": desc},
         "e2e": {"value": v, "unit": "line-evals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -880,6 +954,8 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--conds", type=int, default=40, help="subset of the 40 conditions (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=100.0,
+                    help="--impl reference: seconds of reference CPU work over warm-up + steps")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-server stream")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes, no autotuning")
     ap.add_argument("--serve-rate", type=float, default=200.0)

@@ -12,6 +12,11 @@ bool BaseManager::ReadyForWork() { return true; }
 
 size_t BaseManager::GetNtrans() { return N_trans; }
 
+void BaseManager::SetPrecision(int precision) {
+    if (precision != XS_FP64)
+        throw xs_error(XS_ERR_UNSUPPORTED, "SetPrecision: this manager computes in FP64 only");
+}
+
 // ---------------------------------------------------------------------------
 EngineManager::EngineManager(ProfileType p, int kind, int gpu_id, int num_threads,
                              size_t total_memory)

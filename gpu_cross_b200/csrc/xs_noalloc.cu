@@ -6,23 +6,26 @@
 // cannot afford the implicit device-wide synchronisation that cudaMalloc and
 // cudaFree may cause.  xs_execute_noalloc runs the same kernels as
 // xs_engine_execute -- grid check, step one, persistent step two, and in
-// mixed precision the core pass -- for one condition, but takes its scratch (per-line records and windows, the error
-// word and the work counter) from one fixed array compiled into the library,
+// mixed precision the core pass -- for one condition, but takes its scratch
+// (per-line records and windows, the error word and the work counter) from
+// one fixed array compiled into the library,
 // g_noalloc_scratch below.  It allocates nothing: no cudaMalloc, no cudaFree,
 // no engine, no events, no library routine that allocates.
 //
 // The array is a file-scope __device__ variable, so every GPU that loads the
 // library holds its kXsNoAllocScratchBytes until the process exits.  In host
 // code its name is only a host-side stand-in: the device address comes from
-// cudaGetSymbolAddress, taken once per device, with that device current, by
-// the first call on that device (that first call should therefore come
-// before any stream capture on the device).
+// cudaGetSymbolAddress, with the device current.  Every call looks it up
+// again (a host-side lookup that allocates nothing), so nothing cached goes
+// stale when the caller resets the device or its primary context is torn
+// down and recreated between calls.  The first call on a device may load the
+// library's device code there, so it should come before any stream capture
+// on that device.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "xs_engine.h"
 #include "xs_internal.cuh"
@@ -36,10 +39,6 @@ constexpr size_t kXsNoAllocScratchBytes = size_t(XS_NOALLOC_SCRATCH_BYTES);
 constexpr size_t kHeaderBytes = 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kXsNoAllocScratchBytes];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-void* g_scratch_addr[kMaxDevices] = {};
 
 int noalloc_fail(int code, const char* msg) { return xs::set_error(code, msg); }
 
@@ -92,7 +91,7 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
     }
 
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         cudaGetLastError();
         return noalloc_fail(XS_ERR_NODEVICE, "xs_execute_noalloc: no current CUDA device");
     }
@@ -101,21 +100,16 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
         major != 10)
         return noalloc_fail(XS_ERR_NODEVICE, "xs_execute_noalloc: the kernels are built for sm_100a");
 
-    // One-time set-up on this device (this device is current): the device
-    // address of the fixed array.
+    // The device address of the fixed array on this (current) device, looked
+    // up on every call: after a device reset the module is loaded again and
+    // the array may sit elsewhere.
     void* base_ptr = nullptr;
     {
-        std::lock_guard<std::mutex> lk(g_setup_mu);
-        if (!g_scratch_addr[dev]) {
-            void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess || !p) {
-                cudaGetLastError();
-                return noalloc_fail(XS_ERR_CUDA, "xs_execute_noalloc: cudaGetSymbolAddress failed");
-            }
-            g_scratch_addr[dev] = p;
+        const cudaError_t e = cudaGetSymbolAddress(&base_ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !base_ptr) {
+            cudaGetLastError();
+            return noalloc_fail(XS_ERR_CUDA, "xs_execute_noalloc: cudaGetSymbolAddress failed");
         }
-        base_ptr = g_scratch_addr[dev];
     }
     if (n <= 0 || grid->points <= 0) return XS_OK;
 

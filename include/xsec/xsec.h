@@ -183,8 +183,11 @@ public:
     virtual bool ReadyForWork();
     size_t GetNtrans();
     // Not in the reference: XS_FP64 (default) or XS_MIXED for the step-two
-    // arithmetic of every later ExecuteCrossSection.
-    virtual void SetPrecision(int precision) = 0;
+    // arithmetic of every later ExecuteCrossSection.  Not pure, so that a
+    // BaseManager subclass written against the reference's BaseManager.h:6-33
+    // still compiles: this default accepts XS_FP64 and throws xs_error for
+    // anything else.
+    virtual void SetPrecision(int precision);
 
 protected:
     explicit BaseManager(ProfileType pprofile) : N_trans(0), profile(pprofile) {}

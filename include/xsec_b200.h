@@ -246,8 +246,10 @@ int xs_tune_clear(void);
  * until the process exits.  Line counts whose scratch would not fit (about
  * 320,000 lines for FP64 Voigt, 380,000 for mixed Voigt, 690,000 for
  * Doppler/Gaussian) are rejected with XS_ERR_INVALID before any device work.
- * The first call on a device looks up the array's device address (with that
- * device current); make that first call before any stream capture.  Work is
+ * Every call looks up the array's device address with the device current
+ * (no allocation), so a device reset between calls invalidates nothing the
+ * caller must redo; the first call on a device may load the library's device
+ * code there, so make it before any stream capture on that device.  Work is
  * enqueued on `stream` (cudaStream_t; NULL = legacy) and the call waits for
  * it, then reports XS_ERR_UNSORTED / XS_ERR_GRID like xs_engine_sync.  Every
  * call shares the one array and it keeps the previous call's contents; calls

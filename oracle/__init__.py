@@ -36,7 +36,10 @@ def build(ref: bool = True) -> None:
     """Build liboracle.so, and the reference checkers when the reference
     tree is present."""
     targets = ["oracle"]
-    if ref and os.path.isdir(os.environ.get("REF", "/root/reference")):
+    # the reference tree sits beside the repository checkout unless REF says
+    # otherwise (the same rule as the Makefile's)
+    ref_dir = os.environ.get("REF", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+    if ref and os.path.isdir(ref_dir):
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
 

@@ -284,3 +284,49 @@ def test_compute_without_gpu_fails_loudly(built_libs, tmp_path):
     p = cli(["--input", "case.inp"], tmp_path)
     assert p.returncode == 1 and "device" in p.stderr.lower()
     assert "E+" not in p.stdout and "E-" not in p.stdout
+
+
+# ---------------------------------------------------------------------------
+REF_SIDE_MANAGER = r'''
+#include <cstdio>
+#include "xsec/xsec.h"
+// A manager written against the reference's BaseManager.h:6-33: it defines
+// the reference's pure virtuals only, not SetPrecision.
+class RefSideManager : public BaseManager {
+public:
+    RefSideManager() : BaseManager(VOIGT) {}
+    void InitializeVectors(int) {}
+    void InitializeConstants(double, double, double, double, double, double, double) {}
+    void TransferVectors(size_t, double*, double*, double*, int*, double*, double*) {}
+    void TransferFreq(double*, double*, int) {}
+    void ExecuteCrossSection(int, int, int) {}
+    void TransferResults(double*, double*, int) {}
+    void Cleanup() {}
+};
+int main() {
+    RefSideManager m;
+    BaseManager* b = &m;
+    b->SetPrecision(XS_FP64);
+    try {
+        b->SetPrecision(XS_MIXED);
+    } catch (const xs_error& e) {
+        std::printf("mixed refused: %d\n", e.code());
+        return 0;
+    }
+    return 1;
+}
+'''
+
+
+def test_reference_side_manager_subclass_compiles(built_libs, tmp_path):
+    """BaseManager::SetPrecision is not pure: a subclass with only the
+    reference's virtuals compiles, accepts FP64 and refuses MIXED."""
+    src = tmp_path / "ref_side.cpp"
+    src.write_text(REF_SIDE_MANAGER)
+    exe = tmp_path / "ref_side"
+    libdir = os.path.dirname(build.LIB_HOST)
+    subprocess.run(["g++", "-std=c++11", "-I", build.INCLUDE, str(src), "-o", str(exe), "-L", libdir,
+                    "-lxsec_host", "-lxsec_b200", f"-Wl,-rpath,{libdir}"], check=True, timeout=120)
+    p = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert "mixed refused" in p.stdout

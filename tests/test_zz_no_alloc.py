@@ -68,6 +68,54 @@ def test_noalloc_matches_engine_two_calls_in_a_row(cuda, precision, bound):
         eng.close()
 
 
+# (profile, convention, precision): the other branches of the entry point --
+# the erf profiles and the CPU convention, whose line coverage rule trims the
+# list and whose mixed core pass runs without line splits.
+OTHER_BRANCHES = [
+    (capi.DOPPLER, capi.CONV_GPU, capi.FP64),
+    (capi.DOPPLER, capi.CONV_CPU, capi.FP64),
+    (capi.GAUSSIAN, capi.CONV_GPU, capi.FP64),
+    (capi.VOIGT, capi.CONV_CPU, capi.FP64),
+    (capi.VOIGT, capi.CONV_CPU, capi.MIXED),
+]
+
+
+@pytest.mark.parametrize("profile,convention,precision", OTHER_BRANCHES)
+def test_noalloc_other_branches_match_engine(cuda, profile, convention, precision):
+    import torch
+
+    stream = torch.cuda.current_stream(cuda)
+    eng = capi.Engine(0)
+    eng.set_stream(stream.cuda_stream)
+    bound = MIXED_REL if precision == capi.MIXED else FP64_REL
+    try:
+        cases = []
+        for seed, n, t, p in ((303, 4000, 800.0, 1.0), (404, 2500, 1500.0, 0.3)):
+            lines, grid, cond = _case(seed, n, t, p)
+            d = to_device(lines, cuda)
+            fr = torch.as_tensor(grid.freq(), device=cuda)
+            opts = capi.make_options(profile, grid.dfreq, 17.03, convention=convention,
+                                     precision=precision, cpu_threads=3, half_width=0.05)
+            L = capi.make_lines(d)
+            G = capi.make_grid(fr)
+            ref = torch.zeros_like(fr)
+            eng.execute(opts, [cond], L, G, ref.data_ptr())
+            eng.sync()
+            cases.append((d, fr, opts, cond, L, G, ref))  # d keeps the line arrays alive
+        outs = []
+        for d, fr, opts, cond, L, G, ref in cases:
+            got = torch.zeros_like(fr)
+            _call_noalloc(opts, cond, L, G, got, stream.cuda_stream)
+            outs.append(got)
+        for (d, fr, opts, cond, L, G, ref), got in zip(cases, outs):
+            want = ref.cpu().numpy()
+            assert np.abs(want).max() > 0.0
+            r, a, _ = parity_errors(got.cpu().numpy(), want)
+            assert r <= bound and a <= bound, (r, a)
+    finally:
+        eng.close()
+
+
 def test_noalloc_rejects_oversize_before_device_work(cuda):
     import torch
 
