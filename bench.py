@@ -120,6 +120,24 @@ def pairs_cpu_window(nu: np.ndarray, f0: float, df: float, npts: int, cut: float
     return int(np.sum(np.maximum(ie - ib, 0)))
 
 
+def pairs_doppler_evaluated(nu: np.ndarray, freq: np.ndarray, cut: float, temperature: float,
+                            mass: float) -> int:
+    """Pairs the Doppler kernel actually evaluates: the reference window
+    narrowed to the span where the two erf arguments are not both beyond 6
+    on one side (those pairs add exactly 0 in FP64 and are skipped), with the
+    margins step one uses."""
+    kb, c, na = 1.380658e-16, 2.99792458e10, 6.0221412927e23
+    dpw = np.sqrt(2.0 * kb * temperature * na / mass) / c
+    f0, df, n = freq[0], freq[1] - freq[0], len(freq)
+    lo = np.searchsorted(freq, nu - cut, side="left")
+    hi = np.searchsorted(freq, nu + cut, side="right")
+    w = 6.0 * dpw * (1.0 + 1e-6)
+    m = 0.5 * df * (1.0 + 1e-6) + 2.0 * df
+    alo = np.clip(np.floor((nu * (1.0 - w) - m - f0) / df), 0, n)
+    ahi = np.clip(np.ceil((nu * (1.0 + w) + m - f0) / df) + 1.0, 0, n)
+    return int(np.sum(np.maximum(np.minimum(hi, ahi) - np.maximum(lo, alo), 0)))
+
+
 # --------------------------------------------------------------------------
 # clocks
 # --------------------------------------------------------------------------
@@ -467,6 +485,18 @@ def run_ours(args, rank, world, dist):
     e2e_ms = max_over_ranks(s0.elapsed_time(s1) / e2e_steps) if e2e_steps else float("nan")
     e2e_value = pairs_step * world / (e2e_ms * 1e-3) if e2e_steps else None
 
+    # error statement of the mixed result: the a-priori bound and a sampled
+    # FP64 re-evaluation of 8 rows per condition (one execute outside the
+    # timed region)
+    o_chk = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.MIXED,
+                              ref_temp=common["ref_temp"], check_rows=8)
+    out.zero_()
+    eng.execute(o_chk, cc, L, G, out.data_ptr(), npts)
+    error_statement = eng.accuracy()
+    error_statement["how"] = ("bound_rel: a-priori bound (every grid point and the band integral); "
+                              "sampled_*: FP64 re-evaluation of 8 evenly spaced 32-point rows per "
+                              "condition in the same call, worst over conditions")
+
     step2_ms = float(np.mean(step2))
     achieved = pairs_step * FLOPS_PER_PAIR / (step2_ms * 1e-3) / 1e12
     traffic = xu_pct = None
@@ -549,7 +579,10 @@ def run_ours(args, rank, world, dist):
                                                  "conditions_per_warp": args.C or "auto"},
         },
         "accuracy_vs_fp64": {"max_rel_above_1e-6_peak": rel_max, "max_integrated_rel": integ_max},
-        "fp64": {"value": f64_value, "ms_per_step": f64_step, "unit": "line-evals/s"},
+        "error_statement": error_statement,
+        "grid_points_per_s": npts * nc * world / (ms_step * 1e-3),
+        "fp64": {"value": f64_value, "ms_per_step": f64_step, "unit": "line-evals/s",
+                 "grid_points_per_s": npts * nc * world / (f64_step * 1e-3) if f64_ms else None},
         "speedup_mixed_vs_fp64": value / f64_value if f64_value else None,
         "kernel_ms": {"steptwo_mean": step2_ms, "prep_mean": float(np.mean(prep))},
         "roofline": {
@@ -564,7 +597,8 @@ def run_ours(args, rank, world, dist):
         "cpu_baseline": cpu,
         "reference_gpu_kernel": ref_gpu,
         "e2e": {"value": e2e_value, "unit": "line-evals/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "grid_points_per_s": npts * nc * world / (e2e_ms * 1e-3) if e2e_steps else None},
         "serving": serving,
         "gpu_launches": mix_kernels * args.steps,
         "clocks": clk,
@@ -625,7 +659,9 @@ def run_doppler(args, rank, world, dist):
             out_host.copy_(out, non_blocking=True)
         s1.record(stream)
         torch.cuda.synchronize(dev)
-        res[cut] = dict(pairs=pairs, ms=ms, e2e_ms=s0.elapsed_time(s1) / 2, kernels=g.kernel_count())
+        res[cut] = dict(pairs=pairs, ms=ms, e2e_ms=s0.elapsed_time(s1) / 2, kernels=g.kernel_count(),
+                        evaluated=pairs_doppler_evaluated(lines.nu, fr, cut, cond["temperature"],
+                                                          cond["mean_mass"]))
         g.close()
     eng.close()
     # the reference OpenMPManager (unmodified: cut 100) on a slice, and the
@@ -668,8 +704,12 @@ def run_doppler(args, rank, world, dist):
                                 "T 296 K, Q 2844, M 30.01, grid 0-10000 at 0.01 (1e6 points), cut 25, FP64"),
                    "lines": len(lines), "grid_points": grid.npoints,
                    "line_evals_per_step": res[25.0]["pairs"]},
+        "evaluated_pairs_per_s": res[25.0]["evaluated"] * world / (res[25.0]["ms"] * 1e-3),
+        "evaluated_pairs_per_step": res[25.0]["evaluated"],
+        "grid_points_per_s": grid.npoints * world / (res[25.0]["ms"] * 1e-3),
         "cut_100": {"value": res[100.0]["pairs"] * world / (res[100.0]["ms"] * 1e-3),
-                    "ms_per_step": res[100.0]["ms"], "line_evals_per_step": res[100.0]["pairs"]},
+                    "ms_per_step": res[100.0]["ms"], "line_evals_per_step": res[100.0]["pairs"],
+                    "evaluated_pairs_per_s": res[100.0]["evaluated"] * world / (res[100.0]["ms"] * 1e-3)},
         "cpu_baseline": cpu,
         "e2e": {"value": res[25.0]["pairs"] * world / (res[25.0]["e2e_ms"] * 1e-3),
                 "unit": "line-evals/s", "ms_per_step": res[25.0]["e2e_ms"],
@@ -783,6 +823,7 @@ def run_stream(args, rank, world, dist):
         "accuracy_vs_fp64": {"max_rel_above_1e-6_peak": rel, "max_integrated_rel": integ},
         "fp64": {"ms_per_step": f64["total_ms"], "value": pairs / (f64["total_ms"] * 1e-3),
                  "unit": "line-evals/s"},
+        "grid_points_per_s": grid.npoints * world / (ms * 1e-3),
         "h2d": {"bytes_per_step": h2d, "copy_span_ms": copy_ms,
                 "gb_per_s_over_copy_span": h2d / (copy_ms * 1e-3) / 1e9},
         "e2e": {"value": pairs * world / (e2e_ms * 1e-3), "unit": "line-evals/s",
@@ -878,6 +919,50 @@ def run_serving(args, dev_index: int):
     return res
 
 
+def run_extra_configs(args, rank, world, dist) -> dict:
+    """The other configurations as extra keys of the default run, each with
+    its own timing: "single" (1e7 lines, 7.5e5 points, T 1000 K, P 1 bar;
+    mixed and plain FP64) and "doppler" (the ExoMol-style 1e6-line list,
+    FP64, cut 25 and the reference's 100)."""
+    import copy
+
+    out = {}
+    a = copy.copy(args)
+    a.steps, a.warmup = min(args.steps, 10), 3
+    a.no_serve = a.no_ref_gpu = True
+    a.no_tune = False
+    a.P = a.W = a.C = a.C64 = a.S = 0
+    a.no_cpu = True
+    try:
+        a1 = copy.copy(a)
+        a1.workload, a1.points, a1.lines = "single", 750_000, 10_000_000
+        r = run_ours(a1, rank, world, dist)
+        if r is not None:
+            out["single"] = {k: r.get(k) for k in (
+                "value", "unit", "ms_per_step", "grid_points_per_s", "fp64", "speedup_mixed_vs_fp64",
+                "accuracy_vs_fp64", "error_statement", "kernel_ms", "e2e", "gpu_launches")}
+            out["single"]["config"] = r["config"]["workload"]
+            out["single"]["launch_shape"] = r["config"]["launch_shape"]
+            out["single"]["roofline_frac"] = r["roofline"]["frac"]
+    except Exception as exc:
+        out["single"] = {"error": f"{type(exc).__name__}: {exc}"}
+    try:
+        a2 = copy.copy(a)
+        a2.workload = "doppler"
+        a2.no_cpu = args.no_cpu
+        a2.cpu_seconds = min(args.cpu_seconds, 6.0)
+        r = run_doppler(a2, rank, world, dist)
+        if r is not None:
+            out["doppler"] = {k: r.get(k) for k in (
+                "value", "unit", "ms_per_step", "line_evals_per_step", "evaluated_pairs_per_s",
+                "evaluated_pairs_per_step", "grid_points_per_s", "cut_100", "cpu_baseline", "e2e",
+                "note", "gpu_launches")}
+            out["doppler"]["config"] = r["config"]["workload"]
+    except Exception as exc:
+        out["doppler"] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference's own OpenMPManager on the host cores; rank 0 only.  A
     step is one bounded sample of the sweep workload: one of its conditions
@@ -958,6 +1043,8 @@ def main():
                     help="--impl reference: seconds of reference CPU work over warm-up + steps")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-server stream")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes, no autotuning")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="default run: leave out the single-point and Doppler configurations")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-scale", type=float, default=1.0,
@@ -990,6 +1077,10 @@ def main():
         res = run_doppler(args, rank, world, dist)
     else:
         res = run_ours(args, rank, world, dist)
+        if args.workload == "sweep" and world == 1 and not args.no_extra:
+            extra = run_extra_configs(args, rank, world, dist)
+            if res is not None:
+                res.update(extra)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

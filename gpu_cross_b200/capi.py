@@ -45,7 +45,14 @@ class Options(ctypes.Structure):
                 ("mean_mass", ctypes.c_double), ("ref_temp", ctypes.c_double),
                 ("half_width", ctypes.c_double), ("dfreq", ctypes.c_double),
                 ("points_per_thread", ctypes.c_int), ("warps_per_block", ctypes.c_int),
-                ("conditions_per_warp", ctypes.c_int), ("line_splits", ctypes.c_int)]
+                ("conditions_per_warp", ctypes.c_int), ("line_splits", ctypes.c_int),
+                ("check_rows", ctypes.c_int)]
+
+
+class Accuracy(ctypes.Structure):
+    _fields_ = [("bound_rel", ctypes.c_double), ("sampled_max_rel", ctypes.c_double),
+                ("sampled_integrated_rel", ctypes.c_double), ("sampled_rows", ctypes.c_int),
+                ("conditions", ctypes.c_int)]
 
 
 class Lines(ctypes.Structure):
@@ -75,7 +82,8 @@ class Request(ctypes.Structure):
 class RequestInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("latency_ms", ctypes.c_double),
                 ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("chunks", ctypes.c_int),
-                ("line_evals", ctypes.c_double), ("lines", ctypes.c_size_t)]
+                ("line_evals", ctypes.c_double), ("lines", ctypes.c_size_t),
+                ("err_bound", ctypes.c_double)]
 
 
 class TuneResult(ctypes.Structure):
@@ -114,6 +122,8 @@ _SIGS = {
     "xs_engine_execute": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _I,
                                ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _SZ]),
     "xs_engine_last_stats": (_I, [_VP, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "xs_engine_accuracy": (_I, [_VP, _VP]),
+    "xs_error_bound": (_D, [_I, _I]),
     "xs_engine_capture": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _I,
                                ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _SZ, _I,
                                ctypes.POINTER(_VP)]),
@@ -154,6 +164,8 @@ _SIGS = {
     "xs_server_pending": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "xs_plan_chunks": (_I, [_VP, _SZ, _D, _D, _I, _D, _D, _SZ, _I, _VP, _VP, _VP, _VP, _VP,
                             ctypes.POINTER(_I)]),
+    "xs_split_grid": (_I, [_VP, _SZ, _D, _D, _I, _D, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                           ctypes.POINTER(_SZ), ctypes.POINTER(_SZ), ctypes.POINTER(_D)]),
 }
 
 _lib: ctypes.CDLL | None = None
@@ -240,6 +252,12 @@ class Engine:
         check(lib().xs_engine_execute(self.h, ctypes.byref(opts), arr, len(conds),
                                       ctypes.byref(lines), ctypes.byref(grid), out_ptr, out_stride))
 
+    def accuracy(self) -> dict:
+        """xs_engine_accuracy: the error statement of the last execute."""
+        a = Accuracy()
+        check(lib().xs_engine_accuracy(self.h, ctypes.byref(a)))
+        return {k: getattr(a, k) for k, _ in Accuracy._fields_}
+
     def autotune(self, opts: Options, conds: list[Condition], lines: Lines, grid: GridC, out_ptr: int,
                  out_stride: int = 0) -> dict:
         arr = (Condition * len(conds))(*conds)
@@ -323,9 +341,10 @@ def make_options(profile: int, dfreq: float, mean_mass: float, convention: int =
                  precision: int = FP64, cpu_threads: int = 1, ref_temp: float = 296.0,
                  half_width: float = 0.1, points_per_thread: int = 0,
                  warps_per_block: int = 0, conditions_per_warp: int = 0,
-                 line_splits: int = 0) -> Options:
+                 line_splits: int = 0, check_rows: int = 0) -> Options:
     return Options(profile, convention, precision, cpu_threads, mean_mass, ref_temp, half_width,
-                   dfreq, points_per_thread, warps_per_block, conditions_per_warp, line_splits)
+                   dfreq, points_per_thread, warps_per_block, conditions_per_warp, line_splits,
+                   check_rows)
 
 
 def make_condition(temperature: float, partition: float, pressure: float = 1.0,
@@ -415,6 +434,21 @@ def plan_chunks(nu, f0: float, df: float, npoints: int, cut: float, max_pairs: f
                                out["points"].ctypes.data, out["l0"].ctypes.data,
                                out["l1"].ctypes.data, out["pairs"].ctypes.data, ctypes.byref(n)))
     return {k: v[:n.value] for k, v in out.items()}
+
+
+def split_grid(nu, f0: float, df: float, npoints: int, cut: float, nranks: int, rank: int):
+    """Rank `rank`'s share of a grid-range split (xs_split_grid) on a host nu
+    array: dict(start, points, l0, l1, pairs)."""
+    import numpy as np
+
+    nu = np.ascontiguousarray(nu, dtype=np.float64)
+    st, pt = ctypes.c_int(), ctypes.c_int()
+    a, b = ctypes.c_size_t(), ctypes.c_size_t()
+    pr = ctypes.c_double()
+    check(lib().xs_split_grid(nu.ctypes.data if nu.size else None, nu.size, f0, df, npoints, cut,
+                              nranks, rank, ctypes.byref(st), ctypes.byref(pt), ctypes.byref(a),
+                              ctypes.byref(b), ctypes.byref(pr)))
+    return dict(start=st.value, points=pt.value, l0=a.value, l1=b.value, pairs=pr.value)
 
 
 class Server:

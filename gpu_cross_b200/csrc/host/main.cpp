@@ -1,10 +1,13 @@
 // xsec_cross: the reference's main (main.cpp:17-44) on the B200 engine.
 //
-//   xsec_cross [--input FILE] [--output FILE] [--backend hybrid|gpu|openmp|multigpu]
-//              [--precision fp64|mixed] [--settings] [--list-lines]
+//   xsec_cross [--input FILE] [--output FILE] [--format text|binary]
+//              [--backend hybrid|gpu|openmp|multigpu] [--precision fp64|mixed]
+//              [--settings] [--list-lines]
 //
 // Reads the .inp keyword file (stdin by default), computes the cross-section
-// and prints "%12.6f %13.8E" per grid point, like the reference.  Progress
+// and prints "%12.6f %13.8E" per grid point, like the reference; with
+// --format binary it writes BaseProfile::OutputProfileBinary's layout
+// instead ("XSECBIN1", int64 N, N FP64 wavenumbers, N FP64 values).  Progress
 // goes to stderr.  --settings prints the parsed input and --list-lines the
 // lines the readers return (nu, gns, E'', A, gamma, n), both without a GPU.
 #include <cstdio>
@@ -20,7 +23,7 @@ namespace {
 
 int usage() {
     std::fprintf(stderr,
-                 "usage: xsec_cross [--input FILE] [--output FILE] "
+                 "usage: xsec_cross [--input FILE] [--output FILE] [--format text|binary] "
                  "[--backend hybrid|gpu|openmp|multigpu] [--precision fp64|mixed] "
                  "[--settings] [--list-lines]\n");
     return 2;
@@ -78,7 +81,7 @@ void list_lines(Input& in) {
 int main(int argc, char** argv) {
     std::string input_path, output_path, backend = "hybrid";
     int precision = XS_FP64;
-    bool settings = false, lines = false;
+    bool settings = false, lines = false, binary = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto next = [&]() -> std::string {
@@ -92,6 +95,13 @@ int main(int argc, char** argv) {
                 output_path = next();
             else if (a == "--backend")
                 backend = next();
+            else if (a == "--format") {
+                const std::string f = next();
+                if (f == "binary")
+                    binary = true;
+                else if (f != "text")
+                    return usage();
+            }
             else if (a == "--precision") {
                 const std::string p = next();
                 if (p == "fp64")
@@ -136,12 +146,21 @@ int main(int argc, char** argv) {
         profile->ExecuteCrossSection();
         FILE* out = stdout;
         if (!output_path.empty()) {
-            out = std::fopen(output_path.c_str(), "w");
+            out = std::fopen(output_path.c_str(), binary ? "wb" : "w");
             if (!out) throw xs_error(XS_ERR_INVALID, "cannot write " + output_path);
         }
-        profile->OutputProfile(out);
+        if (binary)
+            profile->OutputProfileBinary(out);
+        else
+            profile->OutputProfile(out);
         if (out != stdout) std::fclose(out);
         std::fprintf(stderr, "%zu lines in %d chunks\n", profile->LinesUsed(), profile->Chunks());
+        // the error statement of the result against the FP64 arithmetic
+        std::fprintf(stderr,
+                     "error bound (%s): every grid point and the band integral within %.3e "
+                     "relative of the FP64 result\n",
+                     precision == XS_MIXED && in.profile == VOIGT ? "mixed FP32/FP64" : "FP64",
+                     xs_error_bound(int(in.profile), precision));
     } catch (const xs_error& e) {
         std::fprintf(stderr, "xsec_cross: %s\n", e.what());
         return 1;

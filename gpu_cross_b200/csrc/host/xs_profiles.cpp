@@ -89,6 +89,18 @@ void BaseProfile::OutputProfile(FILE* out) {
     for (int i = 0; i < Npoints; ++i) std::fprintf(out, "%12.6f %13.8E\n", freq[size_t(i)], intens[size_t(i)]);
 }
 
+void BaseProfile::OutputProfileBinary(FILE* out) {
+    std::fill(intens.begin(), intens.end(), 0.0);
+    manager->TransferResults(freq.data(), intens.data(), Npoints);
+    const char magic[8] = {'X', 'S', 'E', 'C', 'B', 'I', 'N', '1'};
+    const int64_t n = Npoints;
+    bool ok = std::fwrite(magic, 1, 8, out) == 8 && std::fwrite(&n, sizeof(n), 1, out) == 1;
+    if (ok && n > 0)
+        ok = std::fwrite(freq.data(), sizeof(double), size_t(n), out) == size_t(n) &&
+             std::fwrite(intens.data(), sizeof(double), size_t(n), out) == size_t(n);
+    if (!ok) throw xs_error(XS_ERR_INVALID, "OutputProfileBinary: write failed");
+}
+
 // ---------------------------------------------------------------------------
 namespace {
 

@@ -69,6 +69,11 @@ struct xs_engine {
     unsigned* d_words = nullptr;  // [0] error bits, [1] work counter
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     bool timed = false;
+    // error statement of the last execute: the a-priori bound and, with
+    // sampled rows, where their statistics are ([c][4] doubles)
+    double bound_rel = 0.0;
+    const double* chk_stats = nullptr;
+    int chk_rows = 0, chk_ncond = 0;
     std::mutex mu;
 };
 
@@ -145,6 +150,13 @@ CondDev make_cond(const xs_options& o, const xs_condition& c) {
         d.cut = o.half_width * 10.0;
     }
     return d;
+}
+
+// A-priori relative error bound of a result against the FP64 path of the
+// same convention (see xs_engine_accuracy).
+double error_bound(int kind, bool mixed) {
+    if (kind == XS_VOIGT && mixed) return 1024.0 * 0x1p-24;
+    return 1e-12;
 }
 
 // Lines the CPU convention covers: OpenMPManager splits N lines into blocks
@@ -283,6 +295,36 @@ int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* c
     return xs::engine_execute(e, opt, conds, ncond, lines, grid, out, out_stride, nullptr);
 }
 
+double xs_error_bound(int profile, int precision) {
+    return error_bound(profile, profile == XS_VOIGT && precision == XS_MIXED);
+}
+
+int xs_engine_accuracy(xs_engine* e, xs_accuracy* acc) {
+    if (!e || !acc) return fail(XS_ERR_INVALID, "xs_engine_accuracy: NULL argument");
+    std::lock_guard<std::mutex> lk(e->mu);
+    acc->bound_rel = e->bound_rel;
+    acc->sampled_max_rel = -1.0;
+    acc->sampled_integrated_rel = -1.0;
+    acc->sampled_rows = 0;
+    acc->conditions = e->chk_ncond;
+    if (e->chk_rows > 0 && e->chk_stats && e->chk_ncond > 0) {
+        DeviceGuard g(e->device);
+        XS_CU(cudaStreamSynchronize(e->stream));
+        std::vector<double> st(size_t(4 * e->chk_ncond));
+        XS_CU(cudaMemcpy(st.data(), e->chk_stats, sizeof(double) * st.size(), cudaMemcpyDeviceToHost));
+        double mx = 0.0, integ = 0.0;
+        for (int c = 0; c < e->chk_ncond; ++c) {
+            mx = std::fmax(mx, st[size_t(4 * c)]);
+            const double sr = st[size_t(4 * c + 1)], sd = st[size_t(4 * c + 2)];
+            if (sr != 0.0) integ = std::fmax(integ, std::fabs(sd) / std::fabs(sr));
+        }
+        acc->sampled_max_rel = mx;
+        acc->sampled_integrated_rel = integ;
+        acc->sampled_rows = e->chk_rows;
+    }
+    return XS_OK;
+}
+
 int xs_engine_last_stats(xs_engine* e, double* prep_ms, double* steptwo_ms) {
     if (!e) return fail(XS_ERR_INVALID, "xs_engine_last_stats: NULL engine");
     if (!e->timed) return fail(XS_ERR_STATE, "xs_engine_last_stats: nothing executed yet");
@@ -325,8 +367,8 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     if (!grid->freq || grid->npoints_total < 1 || grid->start_idx < 0 || grid->points < 0 ||
         long(grid->start_idx) + long(grid->points) > long(grid->npoints_total))
         return fail(XS_ERR_INVALID, "grid chunk outside the grid");
-    if (ncond > 1 && out_stride < size_t(grid->npoints_total))
-        return fail(XS_ERR_INVALID, "out_stride smaller than the grid");
+    if (ncond > 1 && out_stride < size_t(grid->points))
+        return fail(XS_ERR_INVALID, "out_stride smaller than the grid chunk");
     const bool streamed = ov && ov->s32;
     if (streamed && (kind != XS_VOIGT || opt->convention != XS_CONV_GPU || !ov->gl32))
         return fail(XS_ERR_UNSUPPORTED, "precomputed intensities: VOIGT, GPU convention, with gamma");
@@ -465,8 +507,17 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
     }
     const size_t part_off = (plan.need + 255) & ~size_t(255);
-    const size_t need = S > 1 ? part_off + sizeof(double) * size_t(S) * size_t(group) * size_t(grid->points)
-                              : plan.need;
+    const size_t part_end = S > 1 ? part_off + sizeof(double) * size_t(S) * size_t(group) * size_t(grid->points)
+                                  : plan.need;
+    // sampled FP64 check (mixed Voigt): before/ref values and statistics
+    const bool streamed_call = ov && ov->s32;
+    const int tiles32 = (grid->points + 31) / 32;
+    const int nchk = (mixed && kind == XS_VOIGT && !streamed_call && opt->check_rows > 0)
+                         ? std::min(std::min(opt->check_rows, kMaxCheckRows), tiles32)
+                         : 0;
+    const size_t chk_off = (part_end + 255) & ~size_t(255);
+    const size_t chk_bytes = nchk ? sizeof(double) * (size_t(2 * 32 * nchk) + 4) * size_t(ncond) : 0;
+    const size_t need = nchk ? chk_off + chk_bytes : part_end;
 
     void* scratch = nullptr;
     unsigned* words = e->d_words;
@@ -492,6 +543,13 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     }
     if (ov && ov->alloc_only) return XS_OK;
     char* base = static_cast<char*>(scratch);
+    e->bound_rel = error_bound(kind, mixed);
+    e->chk_rows = nchk;
+    e->chk_ncond = ncond;
+    double* chk_before = nchk ? reinterpret_cast<double*>(base + chk_off) : nullptr;
+    double* chk_ref = nchk ? chk_before + size_t(32 * nchk) * size_t(ncond) : nullptr;
+    double* chk_stats = nchk ? chk_ref + size_t(32 * nchk) * size_t(ncond) : nullptr;
+    e->chk_stats = chk_stats;
 
     GridDev G;
     G.freq = grid->freq;
@@ -539,6 +597,19 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
             if (ov && ov->use_consts) {
                 pa.cond[c].cmcoef = ov->cmcoef;
                 pa.cond[c].beta = ov->beta;
+            }
+        }
+        // temperature classes: the first condition with the same constants
+        for (int c = 0; c < nc; ++c) {
+            pa.tclass[c] = c;
+            for (int k = 0; k < c; ++k) {
+                const CondDev& x = pa.cond[c];
+                const CondDev& y = pa.cond[k];
+                if (x.cmcoef == y.cmcoef && x.beta == y.beta && x.partition == y.partition &&
+                    x.tratio == y.tratio && x.dpw == y.dpw) {
+                    pa.tclass[c] = pa.tclass[k];
+                    break;
+                }
             }
         }
         pa.rec = base + plan.off_rec;
@@ -601,6 +672,35 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
             sa.tiles_per_cond = (grid->points + 31) / 32;
             sa.n_items = sa.tiles_per_cond * (nc / CG) * S;
         }
+        CheckArgs ck;
+        if (nchk) {
+            std::memset(&ck, 0, sizeof(ck));
+            ck.L = L;
+            ck.G = G;
+            ck.ncond = nc;
+            ck.conv = opt->convention;
+            for (int c = 0; c < nc; ++c) {
+                ck.cond[c] = pa.cond[c];
+                ck.row[c] = sa.row[c];
+            }
+            ck.out = out;
+            ck.out_stride = out_stride;
+            ck.nrows = nchk;
+            for (int k = 0; k < nchk; ++k) {
+                // evenly spaced rows of 32 points inside the chunk
+                const long mid = long(grid->points) * (2 * k + 1) / (2 * nchk);
+                long r0 = long(grid->start_idx) + mid - 16;
+                if (r0 > long(grid->start_idx) + grid->points - 32) r0 = long(grid->start_idx) + grid->points - 32;
+                if (r0 < grid->start_idx) r0 = grid->start_idx;
+                ck.rows[k] = int(r0);
+            }
+            ck.before = chk_before + size_t(32 * nchk) * size_t(c0);
+            ck.ref = chk_ref + size_t(32 * nchk) * size_t(c0);
+            ck.stats = chk_stats + size_t(4) * size_t(c0);
+            err = launch_check_snapshot(ck, st);
+            if (err != cudaSuccess) return cuda_fail(err, "check snapshot launch");
+            ++launched;
+        }
         const long want = (long(sa.n_items) + W - 1) / W;
         const int blocks = int(std::min<long>(want, long(occ) * e->num_sms));
         err = CG ? launch_steptwo_mc(mixed, CG, W, blocks, sa, st)
@@ -646,6 +746,11 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         if (timing && c0 + nc >= ncond) {
             cudaEventRecordWithFlags(e->ev[2], st, ev_flags);
             e->timed = true;
+        }
+        if (nchk) {  // after the timed kernels: the check is not step two
+            err = launch_check_rows(ck, st);
+            if (err != cudaSuccess) return cuda_fail(err, "check launch");
+            launched += 2;
         }
     }
     if (ov) ov->kernels += launched;
@@ -801,6 +906,7 @@ int xs_engine_autotune(xs_engine* e, const xs_options* opt, const xs_condition* 
         o.points_per_thread = c.P;
         o.warps_per_block = c.W;
         o.conditions_per_warp = c.C;
+        o.check_rows = 0;  // time the computation alone
         double ms = 1e300;
         for (int rep = 0; rep < 2; ++rep) {
             int rc = xs::engine_execute(e, &o, conds, ncond, lines, grid, out, out_stride, nullptr);

@@ -196,6 +196,10 @@ struct PrepArgs {
                         // (LineShX mixed, LineSh64 FP64)
     CoreIv* civ;        // mixed multi-condition: region intervals and
     float2* cyp;        //   (y, pref) per (condition, line), condition-major
+    // Temperature class of each condition: conditions of one class have the
+    // same beta, Q, T_ref/T and Doppler width, so their intensity, Lorentz
+    // temperature power and 1/Doppler width are the same numbers.
+    int tclass[kMaxCond];
 };
 
 struct StepArgs {
@@ -279,6 +283,34 @@ cudaError_t launch_core_mcx(const CoreArgs& a, int ncond, cudaStream_t stream);
 // The same for the single-condition mixed layout (RecV32 records; a.kx set;
 // with line splits it adds to a.part).
 cudaError_t launch_core_v32(const StepArgs& a, int ncond, cudaStream_t stream);
+
+// Sampled FP64 re-evaluation of a mixed-precision Voigt result: for each
+// condition and each of `nrows` sampled rows of 32 grid points, the FP64 sum
+// of the selected convention (the reference's arithmetic: intensity, widths,
+// window and W4 with its region choice), computed directly from the line
+// arrays, then compared with what the call added to `out`.
+constexpr int kMaxCheckRows = 16;
+struct CheckArgs {
+    LinesDev L;
+    GridDev G;
+    int ncond;
+    int conv;
+    CondDev cond[kMaxCond];
+    int row[kMaxCond];      // output row of each condition
+    double* out;
+    size_t out_stride;
+    int nrows;
+    int rows[kMaxCheckRows];  // first grid index of each sampled row
+    double* before;  // [c][k][32]: out at the sampled points before the call
+    double* ref;     // [c][k][32]: the FP64 sums
+    double* stats;   // [c][4]: max relative error (points above 1e-6 of the
+                     // row's peak), sum of ref, sum of (got - ref), peak
+};
+// Copies out at the sampled points into `before` (launched before step two).
+cudaError_t launch_check_snapshot(const CheckArgs& a, cudaStream_t stream);
+// FP64 sums at the sampled points and the per-condition statistics
+// (launched after the call's last kernel).
+cudaError_t launch_check_rows(const CheckArgs& a, cudaStream_t stream);
 
 // Multi-condition step two (Voigt): C conditions per warp, 32 points per warp.
 cudaError_t launch_steptwo_mc(bool mixed, int C, int warps, int blocks, const StepArgs& a,

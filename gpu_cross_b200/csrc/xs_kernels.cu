@@ -30,6 +30,18 @@ namespace {
 // Depth of the per-warp cp.async staging pipeline (groups of 32 records).
 constexpr int kStages = 3;
 
+// Offsets (in Doppler widths) from which a line's every pair takes the
+// per-pair path, x from its FP64 centre ("whole" lines): FP32 offsets and
+// the region-I sums are exact enough below it.
+constexpr double kWholeXMax = 1.0e8;
+// Scale of the shared-reciprocal products in region I (2^-100).  Region-I
+// denominators d = u^2 + 2 y^2 lie in [1.2e4, 1e32] (|x| + y >= 15, and
+// |x| < 1e8 for lines that are not whole), so tau d lies in [1e-26, 79],
+// tau dA dB in [1.2e-22, 7.9e33] and its reciprocal in [1.3e-34, 8e21]: all
+// normal FP32 numbers.
+constexpr float kPairTau = 7.88860905221011805e-31f;
+
+
 // ---------------------------------------------------------------------------
 // Small complex arithmetic for the W4 regions II-IV.
 // ---------------------------------------------------------------------------
@@ -253,7 +265,7 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
         bool whole = false;
         if (MIXED) {
             const double xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
-            whole = !(fabs(m) < 16000000.0) || !(xw < 1.0e8);
+            whole = !(fabs(m) < 16000000.0) || !(xw < kWholeXMax);
         }
         if (whole) {
             clo_d = -3.0e7;
@@ -488,6 +500,153 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
             for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[threadIdx.x][w] > m ? smax[threadIdx.x][w] : m;
             if (m > 0) atomicMax(a.kc + (threadIdx.x ? kMaxCond : 0) + c, m);
         }
+    }
+}
+
+// Step one of the mixed-precision multi-condition layout, one thread per
+// (line, group of C conditions).  The line's data is read once per group;
+// what the group's conditions share -- the window, the nearest grid index,
+// the condition-free offsets (LineShX) -- is computed once; the C conditions
+// follow in order, and a condition of the same temperature class as the one
+// before it (same beta, Q, T_ref/T and Doppler width, set by the host) reuses
+// its intensity, Lorentz temperature power and 1/Doppler width.  The
+// arithmetic of every value is prep_line's (same operations in the same
+// order), so the records are the same bits.  A line's C/2 CondPairX of the
+// group are contiguous and stored one after the other by the same thread,
+// so each warp fills whole sectors of its records.  Blocks are numbered group
+// fastest: the groups of one range of lines run side by side and share its
+// line data in L2.
+template <int CONV, int C>
+__global__ void __launch_bounds__(128) k_prep_group_x(PrepArgs a) {
+    static_assert(C % 2 == 0, "conditions come in pairs");
+    constexpr int NP = C / 2;
+    const int ngroups = a.ncond / C;
+    const long blk = long(blockIdx.x);
+    const int cg = int(blk % ngroups);
+    const long i = (blk / ngroups) * 128 + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ int smax[2][C][4];
+    const bool live = i < a.L.n;
+    const double* F = a.G.freq;
+    const double f0 = F[0];
+    const double df = a.G.df;
+    const int s = a.G.start, e = a.G.start + a.G.points;
+
+    double nu = 0.0, ei = 0.0, aif = 0.0, gns = 0.0, gam = 0.0, nex = 0.0;
+    if (live) {
+        nu = a.L.nu[i];
+        if (cg == 0 && i > 0 && nu < a.L.nu[i - 1]) atomicOr(a.err, kErrUnsorted);
+        ei = a.L.energies[i];
+        aif = a.L.aif[i];
+        gns = double(a.L.gns[i]);
+        gam = a.L.gamma[i];
+        nex = a.L.nexp[i];
+    }
+    const double cut = a.cond[cg * C].cut;  // a group shares its cut
+    double nu_if = nu;
+    if (nu_if == 0) nu_if = 1e-6;
+    double nu_p;
+    int lo = s, hi = s;
+    if (CONV == kConvGpu) {
+        nu_p = nu;  // step two reads the uploaded centre (cross_kernal.cu:951)
+        if (live) {
+            // -cut <= nu - f <= cut (cross_kernal.cu:952-957)
+            lo = find_first(s, e, ceil((nu - cut - f0) / df), [&](int j) { return !(nu - F[j] > cut); });
+            hi = find_first(s, e, ceil((nu + cut - f0) / df), [&](int j) { return nu - F[j] < -cut; });
+        }
+    } else {
+        // OpenMPManager.cpp:196-208
+        nu_p = nu_if;
+        const double rb = round((nu_if - cut - f0) / df);
+        const double re = round((nu_if + cut - f0) / df);
+        lo = clamp_index(rb > double(s) ? rb : double(s), s, e);
+        hi = clamp_index(re < double(e) ? re : double(e), s, e);
+    }
+    const double m = rint((nu_p - f0) / df);
+    const bool far_m = !(fabs(m) < 16000000.0);
+    const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(i);
+    if (live) {
+        if (cg == 0) a.mi[i] = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
+        LineShX ls;
+        ls.m = float(far_m ? 0.0 : m);
+        ls.dfn = float(df / nu_p);
+        ls.rn = float(((nu_p - f0) - m * df) / nu_p);
+        ls.whole = far_m ? 1 : 0;
+        ls.lo = lo;
+        ls.hi = hi;
+        ls.nu = nu_p;
+        reinterpret_cast<LineShX*>(a.lsh)[gi] = ls;
+        a.wlo[gi] = lo;
+        a.whi[gi] = hi;
+    }
+
+    double S = 0.0, pw = 0.0, g = 0.0;
+    int prev_class = -1;
+    CondPairX cp;
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        const int c = cg * C + k;
+        const CondDev& Cd = a.cond[c];
+        int kcl = 0, rch = 0;
+        if (live) {
+            if (a.tclass[c] != prev_class) {
+                prev_class = a.tclass[c];
+                // device_compute_cross_section_voigt_stepone, cross_kernal.cu:775-779
+                // (GPU); OpenMPManager.cpp:196-200 (CPU)
+                S = Cd.cmcoef * aif * gns * kISQRTPI * exp(-Cd.beta * ei) *
+                    (1.0 - exp(-Cd.beta * nu_if)) / (nu_if * nu_if * Cd.partition);
+                if (CONV == kConvGpu && gns == -1) S = aif;
+                pw = pow(Cd.tratio, nex);
+                g = 1.0 / (nu_p * Cd.dpw);  // gammaG, cross_kernal.cu:958
+            }
+            const double gl = gam * Cd.gamma_scale * pw;
+            const double y = gl * g;
+            const double pref = (CONV == kConvCpu && S == 0.0) ? 0.0 : S * g;
+            const double y2 = y * y;
+            const double Pc = pref * kW4C * y;
+            const double xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
+            const bool whole = far_m || !(xw < kWholeXMax);
+            CoreIv iv;
+            region_interval(nu_p, g, y, 15.0, lo, hi, f0, df, iv.lo15, iv.hi15);
+            region_interval(nu_p, g, y, 5.5, lo, hi, f0, df, iv.lo55, iv.hi55);
+            if (iv.lo15 <= iv.hi15) {
+                const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
+                rch = w < 3.0e7 ? int(w) : 30000000;
+            }
+            kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
+            const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
+            a.civ[ci] = iv;
+            a.cyp[ci] = make_float2(float(y), float(pref));
+            const int h = k & 1;
+            cp.Cy[h] = float(y2 - 0.5);
+            cp.D2[h] = float(2.0 * y2);
+            cp.Pc[h] = float(Pc);
+            cp.lo[h] = iv.lo15;
+            cp.hi[h] = iv.hi15;
+            cp.pad[h] = 0;
+            if (h == 1) {
+                float4* dst = reinterpret_cast<float4*>(reinterpret_cast<CondPairX*>(a.rec) + gi * NP + k / 2);
+                const float4* src = reinterpret_cast<const float4*>(&cp);
+#pragma unroll
+                for (int q = 0; q < int(sizeof(CondPairX) / 16); ++q) dst[q] = src[q];
+            }
+        }
+        kcl = __reduce_max_sync(0xffffffffu, kcl);
+        rch = __reduce_max_sync(0xffffffffu, rch);
+        if (lane == 0) {
+            smax[0][k][warp] = kcl;
+            smax[1][k][warp] = rch;
+        }
+    }
+    // block maxima of the core-candidate widths (kc) and of the core pass's
+    // reach (kc + kMaxCond), one atomic each per block and condition
+    __syncthreads();
+    if (threadIdx.x < 2 * C) {
+        const int which = threadIdx.x / C, k = threadIdx.x % C;
+        int mx = 0;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) mx = smax[which][k][w] > mx ? smax[which][k][w] : mx;
+        if (mx > 0) atomicMax(a.kc + (which ? kMaxCond : 0) + cg * C + k, mx);
     }
 }
 
@@ -824,7 +983,35 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             if (MIXED) {
                 const float4* q = reinterpret_cast<const float4*>(&r);
                 const float4 v0 = q[0], v1 = q[1];
-                if constexpr (P % 2 == 0) {
+                if constexpr (P % 4 == 0) {
+                    // rows (p, p+1) and (p+2, p+3) share one reciprocal per
+                    // two line-evals, as region1_ab in k_steptwo_voigt_mcx
+                    // (region I of a line that is not whole: the scaled
+                    // products stay normal, see kPairTau)
+#pragma unroll
+                    for (int p = 0; p < P; p += 4) {
+                        const float2 dA = __fadd2_rn(f2s(v0.x), f2(-jf[p], -jf[p + 1]));
+                        const float2 dB = __fadd2_rn(f2s(v0.x), f2(-jf[p + 2], -jf[p + 3]));
+                        const float2 xA = __ffma2_rn(dA, f2s(v0.z), f2s(v0.y));
+                        const float2 xB = __ffma2_rn(dB, f2s(v0.z), f2s(v0.y));
+                        const float2 uA = __ffma2_rn(xA, xA, f2s(v0.w));
+                        const float2 uB = __ffma2_rn(xB, xB, f2s(v0.w));
+                        const float2 denA = __ffma2_rn(uA, uA, f2s(v1.x));
+                        const float2 denB = __ffma2_rn(uB, uB, f2s(v1.x));
+                        const float2 numA = __ffma2_rn(uA, f2s(v1.y), f2s(v1.y));
+                        const float2 numB = __ffma2_rn(uB, f2s(v1.y), f2s(v1.y));
+                        const float2 aA = __fmul2_rn(denA, f2s(kPairTau));
+                        const float2 bB = __fmul2_rn(denB, f2s(kPairTau));
+                        const float2 q = __fmul2_rn(aA, denB);
+                        const float2 r = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
+                        const float2 accA = __ffma2_rn(numA, __fmul2_rn(bB, r), f2(accf[p], accf[p + 1]));
+                        const float2 accB = __ffma2_rn(numB, __fmul2_rn(aA, r), f2(accf[p + 2], accf[p + 3]));
+                        accf[p] = accA.x;
+                        accf[p + 1] = accA.y;
+                        accf[p + 2] = accB.x;
+                        accf[p + 3] = accB.y;
+                    }
+                } else if constexpr (P % 2 == 0) {
 #pragma unroll
                     for (int p = 0; p < P; p += 2) {
                         const float2 d = __fadd2_rn(f2s(v0.x), f2(-jf[p], -jf[p + 1]));
@@ -1405,6 +1592,31 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         };
         const std::false_type plain;
         const std::true_type guarded;
+        // Region I of two pairs of conditions (A, B) with one reciprocal per
+        // two line-evals: lane h of A and lane h of B share 1 / (tau dA dB),
+        // so 1/dA = (tau dB) / (tau dA dB) and 1/dB = (tau dA) / (tau dA dB)
+        // (kPairTau: every scaled value stays a normal FP32 number for the
+        // region-I pairs of lines that are not whole).  Pairs where `keep`
+        // is false add exactly zero.
+        auto region1_ab = [&](float X2, const CondPairX& rA, const CondPairX& rB, int pA, int pB,
+                              bool keep) {
+            const float4 fA = *reinterpret_cast<const float4*>(&rA.Cy[0]);
+            const float4 fB = *reinterpret_cast<const float4*>(&rB.Cy[0]);
+            const float2 pcA = *reinterpret_cast<const float2*>(&rA.Pc[0]);
+            const float2 pcB = *reinterpret_cast<const float2*>(&rB.Pc[0]);
+            const float2 uA = __ffma2_rn(f2(X2, X2), k2[pA], f2(fA.x, fA.y));
+            const float2 uB = __ffma2_rn(f2(X2, X2), k2[pB], f2(fB.x, fB.y));
+            const float2 dA = __ffma2_rn(uA, uA, f2(fA.z, fA.w));
+            const float2 dB = __ffma2_rn(uB, uB, f2(fB.z, fB.w));
+            const float2 nA = __ffma2_rn(uA, pcA, pcA);
+            const float2 nB = __ffma2_rn(uB, pcB, pcB);
+            const float2 aA = __fmul2_rn(dA, f2s(kPairTau));
+            const float2 bB = __fmul2_rn(dB, f2s(kPairTau));
+            const float2 q = __fmul2_rn(aA, dB);
+            const float2 r = keep ? f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)) : f2(0.0f, 0.0f);
+            acc[pA] = __ffma2_rn(nA, __fmul2_rn(bB, r), acc[pA]);
+            acc[pB] = __ffma2_rn(nB, __fmul2_rn(aA, r), acc[pB]);
+        };
 
         const int ngroups = split_groups(Lb - La, a.splits, split);
         auto gstart = [&](int gi) { return La + 32 * (split + gi * a.splits); };
@@ -1442,8 +1654,14 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
                     const float X = fmaf(s.x - jf, s.y, s.z);
                     const float X2 = X * X;
+                    if constexpr (NP % 2 == 0) {
 #pragma unroll
-                    for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, true, true);
+                        for (int p = 0; p < NP; p += 2)
+                            region1_ab(X2, SC[t * NP + p], SC[t * NP + p + 1], p, p + 1, true);
+                    } else {
+#pragma unroll
+                        for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, true, true);
+                    }
                 }
             };
             // Partial lines away from every core: the window as a lane mask.
@@ -1453,8 +1671,14 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     const bool in = jj >= SL[t].lo && jj < SL[t].hi && jj < t1;
                     const float X = fmaf(s.x - jf, s.y, s.z);
                     const float X2 = X * X;
+                    if constexpr (NP % 2 == 0) {
 #pragma unroll
-                    for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, in, in);
+                        for (int p = 0; p < NP; p += 2)
+                            region1_ab(X2, SC[t * NP + p], SC[t * NP + p + 1], p, p + 1, in);
+                    } else {
+#pragma unroll
+                        for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, in, in);
+                    }
                 }
             };
             // Core candidates: region I outside each condition's interval.
@@ -1722,6 +1946,116 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_erf(StepArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Sampled FP64 re-evaluation (mixed-precision error statement).
+// ---------------------------------------------------------------------------
+__global__ void k_check_snapshot(CheckArgs a) {
+    const int c = blockIdx.y, k = blockIdx.x, lane = threadIdx.x;
+    const int j = a.rows[k] + lane;
+    const bool in = j < a.G.start + a.G.points;
+    a.before[(size_t(c) * a.nrows + k) * 32 + lane] =
+        in ? a.out[size_t(a.row[c]) * a.out_stride + size_t(j)] : 0.0;
+}
+
+// One warp per (sampled row, condition).  The lines whose window may meet the
+// row are taken 32 at a time, lane = line: each lane computes its line's
+// intensity, widths and window in FP64 as step one does for the FP64 path
+// (cross_kernal.cu:758-790 / OpenMPManager.cpp:183-208); then, line by line
+// in order, every lane adds the line's W4 value at its own point (the
+// reference's region choice, w4_re) when the point lies in the line's window.
+template <int CONV>
+__global__ void __launch_bounds__(32) k_check_rows(CheckArgs a) {
+    const int k = blockIdx.x, c = blockIdx.y, lane = threadIdx.x;
+    const CondDev& C = a.cond[c];
+    const double* F = a.G.freq;
+    const double f0 = F[0], df = a.G.df;
+    const int s = a.G.start, e = a.G.start + a.G.points;
+    const int t0 = a.rows[k];
+    const int t1 = t0 + 32 < e ? t0 + 32 : e;
+    const int j = t0 + lane;
+    const bool mine = j < t1;
+    const double fj = F[mine ? j : t1 - 1];
+    const double cut = C.cut;
+    // lines with nu in [F[t0] - cut - 2 df, F[t1 - 1] + cut + 2 df]
+    const double lo_nu = F[t0] - cut - 2.0 * df, hi_nu = F[t1 - 1] + cut + 2.0 * df;
+    const long La = warp_lower_bound(0, a.L.n, lane, [&](long i) { return a.L.nu[i] >= lo_nu; });
+    const long Lb = warp_lower_bound(La, a.L.n, lane, [&](long i) { return a.L.nu[i] > hi_nu; });
+    double acc = 0.0;
+    for (long b = La; b < Lb; b += 32) {
+        const long i = b + lane;
+        double nu_p = 0.0, g = 0.0, y = 0.0, pref = 0.0;
+        int ib = 0, ie = 0;
+        if (i < Lb) {
+            const double nu = a.L.nu[i];
+            const double ei = a.L.energies[i], aif = a.L.aif[i], gns = double(a.L.gns[i]);
+            double nu_if = nu;
+            if (nu_if == 0) nu_if = 1e-6;
+            double S = C.cmcoef * aif * gns * kISQRTPI * exp(-C.beta * ei) *
+                       (1.0 - exp(-C.beta * nu_if)) / (nu_if * nu_if * C.partition);
+            if (CONV == kConvGpu && gns == -1) S = aif;
+            nu_p = CONV == kConvGpu ? nu : nu_if;
+            const double gl = a.L.gamma[i] * C.gamma_scale * pow(C.tratio, a.L.nexp[i]);
+            g = 1.0 / (nu_p * C.dpw);
+            y = gl * g;
+            pref = (CONV == kConvCpu && S == 0.0) ? 0.0 : S * g;
+            if (CONV == kConvCpu) {
+                const double rb = round((nu_if - cut - f0) / df);
+                const double re = round((nu_if + cut - f0) / df);
+                ib = clamp_index(rb > double(s) ? rb : double(s), s, e);
+                ie = clamp_index(re < double(e) ? re : double(e), s, e);
+            }
+        }
+        const int cnt = Lb - b < 32 ? int(Lb - b) : 32;
+        for (int t = 0; t < cnt; ++t) {
+            const double lnu = __shfl_sync(0xffffffffu, nu_p, t);
+            const double lg = __shfl_sync(0xffffffffu, g, t);
+            const double ly = __shfl_sync(0xffffffffu, y, t);
+            const double lp = __shfl_sync(0xffffffffu, pref, t);
+            const int lib = __shfl_sync(0xffffffffu, ib, t);
+            const int lie = __shfl_sync(0xffffffffu, ie, t);
+            const double d = lnu - fj;
+            const bool in = CONV == kConvGpu ? (!(d > cut) && !(d < -cut)) : (j >= lib && j < lie);
+            if (mine && in) acc += lp * w4_re(d * lg, ly);
+        }
+    }
+    a.ref[(size_t(c) * a.nrows + k) * 32 + lane] = mine ? acc : 0.0;
+}
+
+// Per condition: the comparison of what the call added at the sampled
+// points (out after minus out before) with the FP64 sums.
+__global__ void __launch_bounds__(32) k_check_stats(CheckArgs a) {
+    const int c = blockIdx.x, lane = threadIdx.x;
+    const int e = a.G.start + a.G.points;
+    double peak = 0.0;
+    for (int k = 0; k < a.nrows; ++k) {
+        const double r = a.ref[(size_t(c) * a.nrows + k) * 32 + lane];
+        peak = fmax(peak, fabs(r));
+    }
+    for (int o = 16; o > 0; o >>= 1) peak = fmax(peak, __shfl_xor_sync(0xffffffffu, peak, o));
+    double mx = 0.0, sr = 0.0, sd = 0.0;
+    for (int k = 0; k < a.nrows; ++k) {
+        const int j = a.rows[k] + lane;
+        if (j >= e) continue;
+        const size_t q = (size_t(c) * a.nrows + k) * 32 + lane;
+        const double r = a.ref[q];
+        const double got = a.out[size_t(a.row[c]) * a.out_stride + size_t(j)] - a.before[q];
+        if (fabs(r) > 1e-6 * peak) mx = fmax(mx, fabs(got - r) / fabs(r));
+        sr += r;
+        sd += got - r;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        sd += __shfl_xor_sync(0xffffffffu, sd, o);
+    }
+    if (lane == 0) {
+        a.stats[4 * c + 0] = mx;
+        a.stats[4 * c + 1] = sr;
+        a.stats[4 * c + 2] = sd;
+        a.stats[4 * c + 3] = peak;
+    }
+}
+
 // Sums the parts of split tiles in part order and adds them to out.
 __global__ void k_reduce_splits(StepArgs a, int ncond_out) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1883,6 +2217,23 @@ cudaError_t launch_grid_check(const GridDev& g, unsigned* err, cudaStream_t stre
     return cudaGetLastError();
 }
 
+cudaError_t launch_check_snapshot(const CheckArgs& a, cudaStream_t stream) {
+    if (a.nrows <= 0 || a.ncond <= 0) return cudaSuccess;
+    k_check_snapshot<<<dim3(unsigned(a.nrows), unsigned(a.ncond)), 32, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_check_rows(const CheckArgs& a, cudaStream_t stream) {
+    if (a.nrows <= 0 || a.ncond <= 0) return cudaSuccess;
+    const dim3 grid(unsigned(a.nrows), unsigned(a.ncond));
+    if (a.conv == kConvGpu) k_check_rows<kConvGpu><<<grid, 32, 0, stream>>>(a);
+    else k_check_rows<kConvCpu><<<grid, 32, 0, stream>>>(a);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    k_check_stats<<<unsigned(a.ncond), 32, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_reduce_splits(const StepArgs& a, int ncond_out, cudaStream_t stream) {
     if (a.splits <= 1 || a.G.points <= 0 || ncond_out <= 0) return cudaSuccess;
     const long n = long(a.G.points) * ncond_out;
@@ -1893,7 +2244,29 @@ cudaError_t launch_reduce_splits(const StepArgs& a, int ncond_out, cudaStream_t 
 cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaStream_t stream) {
     if (a.L.n <= 0 || a.ncond <= 0) return cudaSuccess;
     const dim3 grid(unsigned((a.L.n + 255) / 256), unsigned(a.ncond));
-    if (kind == kVoigt && mixed && a.group > 0) {
+    if (kind == kVoigt && mixed && a.group > 0 && a.L.s32 == nullptr) {
+        // one thread per (line, group), group fastest
+        const long ngroups = a.ncond / a.group;
+        const long nblk = (a.L.n + 127) / 128 * ngroups;
+        if (a.ncond % a.group != 0 || nblk > long(INT_MAX)) return cudaErrorInvalidValue;
+        const unsigned gx = unsigned(nblk);
+        switch (a.group) {
+            case 2:
+                if (conv == kConvGpu) k_prep_group_x<kConvGpu, 2><<<gx, 128, 0, stream>>>(a);
+                else k_prep_group_x<kConvCpu, 2><<<gx, 128, 0, stream>>>(a);
+                break;
+            case 4:
+                if (conv == kConvGpu) k_prep_group_x<kConvGpu, 4><<<gx, 128, 0, stream>>>(a);
+                else k_prep_group_x<kConvCpu, 4><<<gx, 128, 0, stream>>>(a);
+                break;
+            case 8:
+                if (conv == kConvGpu) k_prep_group_x<kConvGpu, 8><<<gx, 128, 0, stream>>>(a);
+                else k_prep_group_x<kConvCpu, 8><<<gx, 128, 0, stream>>>(a);
+                break;
+            default:
+                return cudaErrorInvalidValue;
+        }
+    } else if (kind == kVoigt && mixed && a.group > 0) {
         const dim3 pgrid(grid.x, unsigned(a.ncond / 2));
         if (conv == kConvGpu) k_prep_pairs<kConvGpu><<<pgrid, 256, 0, stream>>>(a);
         else k_prep_pairs<kConvCpu><<<pgrid, 256, 0, stream>>>(a);

@@ -925,6 +925,7 @@ int xs_server_wait(xs_server* s, unsigned long long id, double* out, int npoints
         info->chunks = int(r->chunks.size());
         info->line_evals = r->pairs;
         info->lines = r->lines;
+        info->err_bound = xs_error_bound(r->opt.profile, r->opt.precision);
     }
     int rc = r->status;
     std::string err = r->error;
@@ -974,6 +975,51 @@ int xs_plan_chunks(const double* nu, size_t n, double f0, double df, int npoints
         if (l1) l1[k] = plan[k].l1;
         if (pairs) pairs[k] = plan[k].pairs;
     }
+    return XS_OK;
+}
+
+int xs_split_grid(const double* nu, size_t n, double f0, double df, int npoints, double cut,
+                  int nranks, int rank, int* start, int* points, size_t* l0, size_t* l1,
+                  double* pairs) {
+    if ((!nu && n) || npoints < 1 || !(df > 0.0) || !(cut > 0.0) || nranks < 1 || rank < 0 ||
+        rank >= nranks || !start || !points || !l0 || !l1)
+        return sfail(XS_ERR_INVALID, "xs_split_grid: bad arguments");
+    for (size_t i = 1; i < n; ++i)
+        if (nu[i] < nu[i - 1]) return sfail(XS_ERR_UNSORTED, "xs_split_grid: nu must be ascending");
+    std::vector<double> cum(n + 1, 0.0);
+    for (size_t i = 0; i < n; ++i) cum[i + 1] = cum[i] + nu[i];
+    LineIndex L;
+    L.nu = nu;
+    L.cum = cum.data();
+    L.n = n;
+    // one plan entry per 256-point tile (a limit no tile fits in)
+    std::vector<ChunkPlan> tiles;
+    plan_chunks(L, f0, df, npoints, cut, cut, 1e-300, SIZE_MAX, tiles);
+    const int nt = int(tiles.size());
+    std::vector<double> acc(size_t(nt) + 1, 0.0);
+    for (int t = 0; t < nt; ++t) acc[size_t(t) + 1] = acc[size_t(t)] + tiles[size_t(t)].pairs;
+    // rank k starts at the first tile whose preceding work reaches k / nranks
+    // of the total (rank 0 at tile 0, the end at the last tile)
+    auto boundary = [&](int k) {
+        if (k <= 0) return 0;
+        if (k >= nranks) return nt;
+        const double want = acc[size_t(nt)] * double(k) / double(nranks);
+        return int(std::lower_bound(acc.begin(), acc.end(), want) - acc.begin());
+    };
+    int tb = boundary(rank), te = boundary(rank + 1);
+    if (te < tb) te = tb;
+    if (tb >= nt || te == tb) {
+        *start = tb < nt ? tiles[size_t(tb)].start : npoints;
+        *points = 0;
+        *l0 = *l1 = 0;
+        if (pairs) *pairs = 0.0;
+        return XS_OK;
+    }
+    *start = tiles[size_t(tb)].start;
+    *points = tiles[size_t(te) - 1].start + tiles[size_t(te) - 1].points - *start;
+    *l0 = tiles[size_t(tb)].l0;
+    *l1 = tiles[size_t(te) - 1].l1;
+    if (pairs) *pairs = acc[size_t(te)] - acc[size_t(tb)];
     return XS_OK;
 }
 

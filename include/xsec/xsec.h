@@ -293,6 +293,11 @@ public:
     virtual void ExecuteCrossSection() = 0;
     // Writes "%12.6f %13.8E" per grid point (BaseProfile.cpp:65-71).
     void OutputProfile(FILE* out = stdout);
+    // Not in the reference: the same grid and cross-section in binary, with
+    // every bit of the FP64 values (the text keeps nine digits).  Layout,
+    // little-endian: the 8 bytes "XSECBIN1", int64 N, double freq[N],
+    // double sigma[N].
+    void OutputProfileBinary(FILE* out);
     const std::vector<double>& Frequencies() const { return freq; }
     const std::vector<double>& Intensities() const { return intens; }
     // Not in the reference: the manager Initialize() makes, "hybrid" (the

@@ -112,6 +112,10 @@ typedef struct {
                          partial sums are added in a fixed order; 1 = never;
                          N = N parts per tile.  The choice depends only on the
                          call's sizes and the device's SM count. */
+    int check_rows;   /* XS_MIXED Voigt: 0 = no check; k > 0 = after the call,
+                         re-evaluate k evenly spaced rows of 32 grid points
+                         per condition (at most 16) in FP64 and compare
+                         (xs_engine_accuracy). */
 } xs_options;
 
 /* Device-resident line list (structure of arrays, ascending nu). */
@@ -185,10 +189,42 @@ int xs_engine_scratch_bytes(xs_engine* e, size_t* bytes);
 size_t xs_scratch_bytes_needed(const xs_options* opt, int ncond, size_t n_lines);
 
 /* For each condition c: out[c*out_stride + j] += sigma_c(f_j) for j in
- * [grid.start_idx, grid.start_idx + grid.points).  Asynchronous on the
- * engine's stream.  All pointers are device pointers. */
+ * [grid.start_idx, grid.start_idx + grid.points).  With several conditions
+ * out_stride must be at least grid.points (rows of a chunk-sized buffer are
+ * addressed by passing out shifted back by start_idx elements).
+ * Asynchronous on the engine's stream.  All pointers are device pointers. */
 int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
                       const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride);
+
+/* Error statement of the last execute (or graph replay), against the FP64
+ * arithmetic of the same reference convention (no counterpart in the
+ * reference, which computes in FP64 only).
+ *   bound_rel: a-priori bound on the relative error of every grid point of
+ *     the result, and so of the band integral (all terms are positive for
+ *     non-negative intensities).  Mixed Voigt: 1024 * 2^-24 = 6.1e-5, twice
+ *     the rounding-error analysis of the FP32 steps (region I: offset, u,
+ *     u^2 + 2y^2, the shared reciprocal, 32-line FP32 partial sums folded
+ *     with compensation; regions II-IV: the FP32 x and y through the
+ *     profile's sensitivity, at most 2 x^2 = 60.5, and the FP32 W4 forms).
+ *     FP64 (every FP64 result, Doppler and Gaussian included): 1e-12,
+ *     summation order only.
+ *   sampled_*: with xs_options.check_rows > 0 (mixed Voigt), measured on
+ *     the sampled rows of every condition -- the largest relative error on
+ *     points above 1e-6 of the rows' FP64 peak, and the relative error of
+ *     their sum -- as the worst over conditions; -1 when not measured.  What
+ *     the call added is taken as out after minus out before the call.
+ * Waits for the engine's stream. */
+typedef struct {
+    double bound_rel;
+    double sampled_max_rel;
+    double sampled_integrated_rel;
+    int sampled_rows;  /* rows per condition measured (0: none) */
+    int conditions;
+} xs_accuracy;
+int xs_engine_accuracy(xs_engine* e, xs_accuracy* acc);
+/* The a-priori bound alone (xs_accuracy.bound_rel) for a profile and
+ * precision: 1024 * 2^-24 for XS_MIXED Voigt, 1e-12 otherwise. */
+double xs_error_bound(int profile, int precision);
 
 /* Device time (ms, CUDA events on the engine's stream) of the step-one
  * (prep) and step-two launches of the last execute; waits for them. */
@@ -358,6 +394,10 @@ typedef struct {
     int chunks;
     double line_evals;  /* sum of window overlaps / df (an estimate) */
     size_t lines;       /* lines within the grid +/- cut */
+    double err_bound;   /* a-priori bound on the relative error of every grid
+                           point and of the band integral against the FP64
+                           arithmetic (xs_error_bound of the request's profile
+                           and precision) */
 } xs_request_info;
 
 int xs_server_create(int device, const xs_server_config* cfg, xs_server** out);
@@ -388,6 +428,19 @@ int xs_server_pending(xs_server* s, int* queued, int* active);
 int xs_plan_chunks(const double* nu, size_t n, double f0, double df, int npoints, double cut,
                    double max_pairs, size_t max_lines, int cap, int* start, int* points,
                    size_t* l0, size_t* l1, double* pairs, int* nchunks);
+/* Grid-range split for several GPUs (no counterpart in the reference, whose
+ * MultiGPUManager.cpp:61-83 shards the transitions and sums whole grids on
+ * the host).  Grid tiles are independent, so rank `rank` of `nranks` takes
+ * the grid points [*start, *start + *points) -- whole 256-point tiles, the
+ * ranges contiguous, in rank order and balanced by estimated line-evals --
+ * and only the lines [*l0, *l1) of the ascending host array `nu` whose
+ * window (+-cut) can reach them.  Each rank computes its slice with no
+ * reduction; the slices are concatenated (gpu_cross_b200.multigpu gathers
+ * them over torch.distributed).  A rank with no work gets *points = 0.
+ * *pairs (may be NULL): the rank's estimated line-evals.  Host only. */
+int xs_split_grid(const double* nu, size_t n, double f0, double df, int npoints, double cut,
+                  int nranks, int rank, int* start, int* points, size_t* l0, size_t* l1,
+                  double* pairs);
 
 #ifdef __cplusplus
 }

@@ -95,3 +95,38 @@ def test_cli_openmp_backend_equals_hybrid(cuda, tmp_path):
     _, a, _ = run_cli(tmp_path)
     _, b, _ = run_cli(tmp_path, "--backend", "openmp")
     np.testing.assert_array_equal(a, b)
+
+
+def read_binary_spectrum(path):
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"XSECBIN1"
+    n = int(np.frombuffer(raw[8:16], dtype="<i8")[0])
+    body = np.frombuffer(raw[16:], dtype="<f8")
+    assert body.size == 2 * n
+    return body[:n], body[n:]
+
+
+@pytest.mark.parametrize("name", ["exomol_doppler", "hitran_voigt"])
+def test_cli_binary_output_keeps_fp64(cuda, tmp_path, name):
+    """--format binary writes every bit of the grid and the cross-section:
+    the GPU-convention backend against the oracle at the FP64 bound (the
+    text output holds nine digits), and the same values as the text."""
+    lines, cond, grid, prof, _ = case_lines(name, tmp_path)
+    p = cli(["--input", "case.inp", "--backend", "gpu", "--format", "binary", "--output",
+             "spec.bin"], tmp_path)
+    assert p.returncode == 0, p.stderr[-2000:]
+    fr, got = read_binary_spectrum(tmp_path / "spec.bin")
+    np.testing.assert_allclose(fr, grid.freq(), rtol=1e-15, atol=0)
+    want = np.zeros(grid.npoints)
+    k = 0
+    for n, ib, ie in chunks_of(p.stderr):
+        if ie > ib:
+            want = oracle.gpu_convention(prof, grid.freq(), want, lines.slice(k, k + n), cond,
+                                         grid.dfreq, points=ie - ib, start_idx=ib)
+        k += n
+    peak = np.abs(want).max()
+    big = np.abs(want) > PEAK_FLOOR * peak
+    assert np.max(np.abs(got[big] - want[big]) / np.abs(want[big])) <= 1e-10
+    assert np.max(np.abs(got[~big] - want[~big]), initial=0.0) <= 1e-10 * peak
+    _, text, _ = run_cli(tmp_path, "--backend", "gpu")
+    assert np.all(np.abs(text - got) <= PRINT_REL * np.abs(got) + 1e-300)

@@ -55,8 +55,15 @@ def test_server_matches_oracle(cuda, molecule, prof, prec):
     want, _ = oracle_for(subset(molecule, f0 - 30, f0 + n * df + 30), prof, T, Q, P, f0, df, n, cut)
     if prec == capi.FP64:
         assert_fp64_parity(got, want, FP64_REL)
+        assert info["err_bound"] <= 1e-12
     else:
         assert_mixed_parity(got, want)
+        # the request's error statement bounds its true error against FP64
+        assert info["err_bound"] == pytest.approx(1024 * 2.0 ** -24)
+        peak = np.abs(want).max()
+        big = np.abs(want) > 1e-6 * peak
+        assert np.max(np.abs(got[big] - want[big]) / np.abs(want[big])) <= info["err_bound"]
+        assert abs(got.sum() - want.sum()) / want.sum() <= info["err_bound"]
 
 
 def random_requests(mid, rng, k):
