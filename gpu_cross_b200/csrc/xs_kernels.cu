@@ -160,6 +160,25 @@ __device__ void region_interval(double nu, double g, double y, double lim, int l
     }
 }
 
+// region_interval with its two starting guesses from precomputed values:
+// md = (nu - f0) / df and q = 1 / (g df) (no division).  The guesses only
+// decide where the walks start; the intervals are the same.
+__device__ __forceinline__ void region_interval_q(double nu, double g, double y, double lim, int lo, int hi, double f0,
+                                  double df, double md, double q, int& jlo, int& jhi) {
+    jlo = 1;
+    jhi = 0;
+    if (!(y < lim) || lo >= hi) return;
+    auto fa = [&](int j) { return fma(double(j), df, f0); };
+    auto inside = [&](int j) { return !(fabs((nu - fa(j)) * g) + y >= lim); };
+    const double hq = (lim - y) * q;
+    const int jl = find_first(lo, hi, ceil(md - hq), [&](int j) { return fa(j) > nu || inside(j); });
+    const int jh = find_first(lo, hi, floor(md + hq) + 1.0, [&](int j) { return fa(j) > nu && !inside(j); });
+    if (jl < jh) {
+        jlo = jl;
+        jhi = jh - 1;
+    }
+}
+
 // `reach` (mixed Voigt): the largest distance, in grid points, from the
 // line's nearest grid index to its region interval (the core pass's reach).
 // `pair`: the mixed-precision multi-condition layout fills its condition's
@@ -517,7 +536,7 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
 // fastest: the groups of one range of lines run side by side and share its
 // line data in L2.
 template <int CONV, int C>
-__global__ void __launch_bounds__(128) k_prep_group_x(PrepArgs a) {
+__global__ void __launch_bounds__(128, 4) k_prep_group_x(PrepArgs a) {
     static_assert(C % 2 == 0, "conditions come in pairs");
     constexpr int NP = C / 2;
     const int ngroups = a.ncond / C;
@@ -562,7 +581,9 @@ __global__ void __launch_bounds__(128) k_prep_group_x(PrepArgs a) {
         lo = clamp_index(rb > double(s) ? rb : double(s), s, e);
         hi = clamp_index(re < double(e) ? re : double(e), s, e);
     }
-    const double m = rint((nu_p - f0) / df);
+    const double md = (nu_p - f0) / df;
+    const double m = rint(md);
+    const double nu_df = nu_p / df;  // q = 1 / (g df) = nu_df * dpw
     const bool far_m = !(fabs(m) < 16000000.0);
     const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(i);
     if (live) {
@@ -607,8 +628,9 @@ __global__ void __launch_bounds__(128) k_prep_group_x(PrepArgs a) {
             const double xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
             const bool whole = far_m || !(xw < kWholeXMax);
             CoreIv iv;
-            region_interval(nu_p, g, y, 15.0, lo, hi, f0, df, iv.lo15, iv.hi15);
-            region_interval(nu_p, g, y, 5.5, lo, hi, f0, df, iv.lo55, iv.hi55);
+            const double q = nu_df * Cd.dpw;
+            region_interval_q(nu_p, g, y, 15.0, lo, hi, f0, df, md, q, iv.lo15, iv.hi15);
+            region_interval_q(nu_p, g, y, 5.5, lo, hi, f0, df, md, q, iv.lo55, iv.hi55);
             if (iv.lo15 <= iv.hi15) {
                 const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
                 rch = w < 3.0e7 ? int(w) : 30000000;
@@ -1043,6 +1065,32 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
                 }
             }
         };
+        // Two full lines away from every core at two rows per thread
+        // (mixed, P == 2): row pair (0, 1) of line A and of line B share one
+        // reciprocal per two line-evals, as region1_ab in
+        // k_steptwo_voigt_mcx; A's terms are added before B's.
+        auto fast_line2 = [&](const REC& rA, const REC& rB) {
+            const float4* qa = reinterpret_cast<const float4*>(&rA);
+            const float4* qb = reinterpret_cast<const float4*>(&rB);
+            const float4 a0 = qa[0], a1 = qa[1], b0 = qb[0], b1 = qb[1];
+            const float2 nj = f2(-jf[0], -jf[1]);
+            const float2 xA = __ffma2_rn(__fadd2_rn(f2s(a0.x), nj), f2s(a0.z), f2s(a0.y));
+            const float2 xB = __ffma2_rn(__fadd2_rn(f2s(b0.x), nj), f2s(b0.z), f2s(b0.y));
+            const float2 uA = __ffma2_rn(xA, xA, f2s(a0.w));
+            const float2 uB = __ffma2_rn(xB, xB, f2s(b0.w));
+            const float2 denA = __ffma2_rn(uA, uA, f2s(a1.x));
+            const float2 denB = __ffma2_rn(uB, uB, f2s(b1.x));
+            const float2 numA = __ffma2_rn(uA, f2s(a1.y), f2s(a1.y));
+            const float2 numB = __ffma2_rn(uB, f2s(b1.y), f2s(b1.y));
+            const float2 aA = __fmul2_rn(denA, f2s(kPairTau));
+            const float2 bB = __fmul2_rn(denB, f2s(kPairTau));
+            const float2 q = __fmul2_rn(aA, denB);
+            const float2 rr = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
+            float2 acc = __ffma2_rn(numA, __fmul2_rn(bB, rr), f2(accf[0], accf[P > 1 ? 1 : 0]));
+            acc = __ffma2_rn(numB, __fmul2_rn(aA, rr), acc);
+            accf[0] = acc.x;
+            accf[P > 1 ? 1 : 0] = acc.y;
+        };
         // `full`: the line's window covers the whole tile.
         auto slow_line = [&](const REC& r, bool full) {
             if (MIXED) {
@@ -1244,14 +1292,22 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             {
                 int t = a1;
                 for (; t + 1 < b1; t += 2) {
-                    fast_line(R[t]);
-                    fast_line(R[t + 1]);
+                    if constexpr (MIXED && P == 2) {
+                        fast_line2(R[t], R[t + 1]);
+                    } else {
+                        fast_line(R[t]);
+                        fast_line(R[t + 1]);
+                    }
                 }
                 if (t < b1) fast_line(R[t]);
                 t = c1;
                 for (; t + 1 < d1; t += 2) {
-                    fast_line(R[t]);
-                    fast_line(R[t + 1]);
+                    if constexpr (MIXED && P == 2) {
+                        fast_line2(R[t], R[t + 1]);
+                    } else {
+                        fast_line(R[t]);
+                        fast_line(R[t + 1]);
+                    }
                 }
                 if (t < d1) fast_line(R[t]);
             }
@@ -1735,6 +1791,32 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
     }
 }
 
+// The core passes' per-warp table: row = point of the 32-point row, column =
+// line of the batch (stride kCoreRow floats keeps rows 16-byte aligned and a
+// quarter-warp's 128-bit row reads on distinct banks).  It starts all zero;
+// each lane writes its line's entries, every lane then sums its point's row in
+// line order, and each lane clears what it wrote.
+constexpr int kCoreRow = 36;
+__device__ __forceinline__ void core_table_clear(float (*T)[kCoreRow], int lane) {
+#pragma unroll
+    for (int q = 0; q < 32; q += 4) *reinterpret_cast<float4*>(&T[lane][q]) = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncwarp();
+}
+// Sum of this lane's row in line order.  Entries of lines that wrote nothing
+// are +0 and leave the (non-negative) sum unchanged.
+__device__ __forceinline__ float core_table_column(float (*T)[kCoreRow], int lane) {
+    float part = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 32; q += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(&T[lane][q]);
+        part += v.x;
+        part += v.y;
+        part += v.z;
+        part += v.w;
+    }
+    return part;
+}
+
 // Core pass of the mixed multi-condition layout.  A warp takes a (condition,
 // row of 32 grid points); the lines whose region interval may reach the row
 // form one run (the nearest grid index mi[] is ascending; the condition's
@@ -1747,13 +1829,15 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
 // row's batches are shared out as in step two and the sums go to the parts.
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
-    __shared__ float tab[WARPS][32][33];  // [line of the batch][point], padded
+    __shared__ __align__(16) float tab[WARPS][32][kCoreRow];  // [point][line of the batch]
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int c = int(blockIdx.y);
     const int t0 = a.G.start + (int(blockIdx.x) * WARPS + warp) * 32;
     const int end = a.G.start + a.G.points;
     if (t0 >= end) return;
+    float (*T)[kCoreRow] = tab[warp];
+    core_table_clear(T, lane);
     const int t1 = t0 + 32 < end ? t0 + 32 : end;
     const int tl = t1 - 1;
     const int K = a.kc[kMaxCond + c];  // the condition's core-pass reach
@@ -1763,16 +1847,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     const float2* cyp = a.cyp + size_t(c) * size_t(a.n);
     const LineShX* lsh = a.lsh + size_t(c / a.group) * size_t(a.n);
     const float k = a.kx[c];
-    float (*T)[33] = tab[warp];
     const int split = int(blockIdx.z), S = a.splits;
     double acc = 0.0;
     for (long b = E + 32L * split; b < F; b += 32L * S) {
-#pragma unroll
-        for (int q = 0; q < 32; ++q) T[lane][q] = 0.0f;
         const long i = b + lane;
+        int jlo = 1, jhi = 0;
         if (i < F) {
             const CoreIv iv = civ[i];
-            const int jlo = max(iv.lo15, t0), jhi = min(iv.hi15, tl);
+            jlo = max(iv.lo15, t0);
+            jhi = min(iv.hi15, tl);
             if (jlo <= jhi) {
                 const LineShX s = lsh[i];
                 const float2 yp = cyp[i];
@@ -1784,16 +1867,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
                         w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y) : w4_region4_re_f32(ax, y);
                     else
                         w = w4_region2_re<float>(ax, y);
-                    T[lane][j - t0] = yp.y * w;
+                    T[j - t0][lane] = yp.y * w;
                 }
             }
         }
         __syncwarp();
-        const long nb = F - b < 32 ? F - b : 32;
-        float part = 0.0f;
-        for (int t = 0; t < int(nb); ++t) part += T[t][lane];
-        acc += double(part);
+        acc += double(core_table_column(T, lane));
         __syncwarp();
+        for (int j = jlo; j <= jhi; ++j) T[j - t0][lane] = 0.0f;  // back to all zeros
     }
     const int jj = t0 + lane;
     if (jj < t1) {
@@ -1809,13 +1890,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
 // line marked whole (dfa < 0) takes x from its FP64 centre.
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_core_v32(StepArgs a) {
-    __shared__ float tab[WARPS][32][33];  // [line of the batch][point], padded
+    __shared__ __align__(16) float tab[WARPS][32][kCoreRow];  // [point][line of the batch]
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int c = int(blockIdx.y);
     const int t0 = a.G.start + (int(blockIdx.x) * WARPS + warp) * 32;
     const int end = a.G.start + a.G.points;
     if (t0 >= end) return;
+    float (*T)[kCoreRow] = tab[warp];
+    core_table_clear(T, lane);
     const int t1 = t0 + 32 < end ? t0 + 32 : end;
     const int tl = t1 - 1;
     const int K = a.kc[kMaxCond + c];  // the condition's core-pass reach
@@ -1823,17 +1906,16 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_v32(StepArgs a) {
     const long F = warp_lower_bound(E, a.n, lane, [&](long i) { return a.mi[i] > tl + K; });
     const RecV32* recs = reinterpret_cast<const RecV32*>(a.rec) + size_t(c) * size_t(a.n);
     const float k = a.kx[c];
-    float (*T)[33] = tab[warp];
     const int split = int(blockIdx.z), S = a.splits;
     double acc = 0.0;
     for (long b = E + 32L * split; b < F; b += 32L * S) {
-#pragma unroll
-        for (int q = 0; q < 32; ++q) T[lane][q] = 0.0f;
         const long i = b + lane;
+        int jlo = 1, jhi = 0;
         if (i < F) {
             const RecV32 r = recs[i];
             const bool whole = r.dfa < 0.0f;
-            const int jlo = max(int(r.clo), t0), jhi = min(int(r.chi), tl);
+            jlo = max(int(r.clo), t0);
+            jhi = min(int(r.chi), tl);
             for (int j = jlo; j <= jhi; ++j) {
                 const float xs = whole ? float((r.nu - a.G.freq[j]) / r.nu) * k : fmaf(r.m - float(j), r.dfa, r.ra);
                 const float ax = fabsf(xs), y = r.y;
@@ -1842,15 +1924,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_v32(StepArgs a) {
                     w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y) : w4_region4_re_f32(ax, y);
                 else
                     w = w4_region2_re<float>(ax, y);
-                T[lane][j - t0] = r.pref * w;
+                T[j - t0][lane] = r.pref * w;
             }
         }
         __syncwarp();
-        const long nb = F - b < 32 ? F - b : 32;
-        float part = 0.0f;
-        for (int t = 0; t < int(nb); ++t) part += T[t][lane];
-        acc += double(part);
+        acc += double(core_table_column(T, lane));
         __syncwarp();
+        for (int j = jlo; j <= jhi; ++j) T[j - t0][lane] = 0.0f;  // back to all zeros
     }
     const int jj = t0 + lane;
     if (jj < t1) {
