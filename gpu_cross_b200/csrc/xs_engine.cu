@@ -273,6 +273,10 @@ int xs_engine_sync(xs_engine* e) {
                                          "requires nu-sorted input)");
         if (w & kErrGrid)
             return fail(XS_ERR_GRID, "the grid is not ascending with the uniform step dfreq");
+        if (w & kErrReach)
+            return fail(XS_ERR_UNSUPPORTED, "mixed precision: a line's core lies 3e7 or more grid points "
+                                            "from its centre's grid index (grid step too fine for the "
+                                            "cut); use FP64");
     }
     return XS_OK;
 }

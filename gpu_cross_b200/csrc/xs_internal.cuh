@@ -35,6 +35,10 @@ enum Conv : int { kConvGpu = 0, kConvCpu = 1 };
 // Device-side error bits (OR-ed into the engine's error word).
 constexpr unsigned kErrUnsorted = 1u;
 constexpr unsigned kErrGrid = 2u;
+// A line's W4 region interval lies 3e7 or more grid points from the grid
+// index of its centre (mixed precision; a grid step far below the cut over
+// 3e7): the core pass, which finds lines by that index, could miss it.
+constexpr unsigned kErrReach = 4u;
 
 constexpr int kMaxCond = 64;  // conditions per launch (the sweep uses 40)
 constexpr int kMaxSplits = 64;                      // line splits per tile

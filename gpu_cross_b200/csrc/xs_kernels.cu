@@ -324,6 +324,7 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
                 if (iv.lo15 <= iv.hi15) {
                     const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
                     rch = w < 3.0e7 ? int(w) : 30000000;
+                    if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
                 }
                 if (reach) *reach = rch;
                 // a whole line is a core candidate of every tile
@@ -396,6 +397,7 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
             if (j15 <= k15) {
                 const double w = fmax(m - double(j15), double(k15) - m);
                 rch = w < 3.0e7 ? int(w) : 30000000;
+                if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
             }
             if (reach) *reach = rch;
             kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
@@ -634,6 +636,7 @@ __global__ void __launch_bounds__(128, 4) k_prep_group_x(PrepArgs a) {
             if (iv.lo15 <= iv.hi15) {
                 const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
                 rch = w < 3.0e7 ? int(w) : 30000000;
+                if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
             }
             kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
             const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);

@@ -207,5 +207,8 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
         return noalloc_fail(XS_ERR_UNSORTED, "xs_execute_noalloc: line centres not ascending");
     if (bits & xs::kErrGrid)
         return noalloc_fail(XS_ERR_GRID, "xs_execute_noalloc: grid not ascending/uniform");
+    if (bits & xs::kErrReach)
+        return noalloc_fail(XS_ERR_UNSUPPORTED, "xs_execute_noalloc: a line's core lies too far from "
+                                                "its centre's grid index for mixed precision");
     return XS_OK;
 }

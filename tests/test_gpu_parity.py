@@ -265,6 +265,25 @@ def test_unsorted_lines_are_reported(engine, cuda):
     assert ei.value.code == capi.XS_ERR_UNSORTED
 
 
+@pytest.mark.parametrize("C", [1, 2])
+def test_unreachable_core_is_reported_in_mixed(engine, cuda, C):
+    """A grid so fine (5e-10 cm-1) that a line's core reaches it from 4e7
+    grid points away: the mixed core pass finds lines by the grid index of
+    their centre within a bounded reach, so the engine reports
+    XS_ERR_UNSUPPORTED instead of leaving those pairs out; FP64 computes it."""
+    grid = synth.Grid(1000.0, 1000.0 + 1000 * 5e-10, 1000)
+    line = synth.random_lines(1, 999.98, 999.98 + 1e-9, 100.0, 1.0, 1.0001, seed=5)
+    conds = [dict(temperature=2000.0, partition=synth.partition_poly(2000.0), mean_mass=17.03,
+                  pressure=1.0, cut=25.0, gamma_scale=s) for s in (1e-4, 2e-4)]
+    f64 = run_engine(engine, capi.VOIGT, line, grid.freq(), conds[0], grid.dfreq, cuda,
+                     conds=conds, C=C if C > 1 else 0)
+    assert np.all(f64 > 0.0)
+    with pytest.raises(capi.XsError) as ei:
+        run_engine(engine, capi.VOIGT, line, grid.freq(), conds[0], grid.dfreq, cuda,
+                   conds=conds, C=C if C > 1 else 1, precision=capi.MIXED)
+    assert ei.value.code == capi.XS_ERR_UNSUPPORTED
+
+
 def test_bad_arguments_rejected(engine, cuda):
     lines, grid, cond = small_voigt_case(seed=2, n=10)
     with pytest.raises(capi.XsError) as ei:
