@@ -47,6 +47,11 @@ def test_voigt_shapes_agree(engine, cuda, P):
     for W in (4, 8):
         got = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, P=P, W=W)
         assert_fp64_parity(got, ref)
+        # the mixed kernel at this shape (P = 2, 4, 8: reciprocals shared
+        # between two lines or two row pairs)
+        mix = run_engine(engine, capi.VOIGT, lines, fr, cond, grid.dfreq, cuda, P=P, W=W,
+                         precision=capi.MIXED)
+        assert_mixed_parity(mix, ref)
 
 
 @pytest.mark.parametrize("S", [1, 3, 64])
@@ -86,6 +91,27 @@ def test_line_splits_multi_condition(engine, cuda):
     for k in range(len(conds)):
         assert_mixed_parity(one[k], f64[k])
         assert_mixed_parity(five[k], f64[k])
+
+
+@pytest.mark.parametrize("C", [2, 4, 8])
+def test_multi_condition_mixed_cpu_convention(engine, cuda, C):
+    """Mixed multi-condition tiles in the CPU convention (sqrt(ln 2) Doppler
+    widths, rounded windows, the OpenMPManager's line coverage) against the
+    oracle's OpenMPManager restatement, per condition."""
+    lines = synth.random_lines(3000, 1000.0, 1100.0, 2500.0, 1e-6, 1e2, seed=53, pressure_atm=1.0)
+    grid = synth.Grid(990.0, 1110.0, 1200)
+    base = dict(mean_mass=17.03, pressure=1.0, ref_temp=296.0)
+    conds = [dict(base, temperature=t, partition=synth.partition_poly(t), gamma_scale=p)
+             for t in (300.0, 700.0, 1500.0, 2100.0) for p in (1e-3, 10.0)]
+    fr = grid.freq()
+    mix = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, C=C,
+                     convention=capi.CONV_CPU, cpu_threads=3, precision=capi.MIXED)
+    for k, c in enumerate(conds):
+        scaled = synth.LineList(lines.nu, lines.energies, lines.aif, lines.gns,
+                                lines.gamma * c["gamma_scale"], lines.n)
+        ref = oracle.cpu_convention(oracle.VOIGT, fr, np.zeros_like(fr), scaled,
+                                    dict(c, pressure=1.0), grid.dfreq, nthreads=3)
+        assert_mixed_parity(mix[k], ref)
 
 
 @pytest.mark.parametrize("threads", [1, 3, 8])
