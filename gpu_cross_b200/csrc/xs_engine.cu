@@ -633,6 +633,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.lsh = base + plan.off_lsh;
         pa.civ = reinterpret_cast<CoreIv*>(base + plan.off_civ);
         pa.cyp = reinterpret_cast<float2*>(base + plan.off_cyp);
+        pa.liv = reinterpret_cast<int*>(base + plan.off_liv);
 
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, ev_flags);
         err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(2 * kMaxCond), st);
@@ -672,6 +673,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
         if (CG) {
             sa.lsh = pa.lsh;
+            sa.liv = pa.liv;
             sa.group = CG;
             sa.tiles_per_cond = (grid->points + 31) / 32;
             sa.n_items = sa.tiles_per_cond * (nc / CG) * S;

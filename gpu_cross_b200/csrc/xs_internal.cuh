@@ -115,19 +115,31 @@ struct __align__(16) LineShX {
     double nu;    // centre (whole lines)
 };
 static_assert(sizeof(LineShX) == 32, "LineShX layout");
-// Conditions 2k and 2k+1 of a group side by side, so that each pair of
-// values is one packed FP32x2 operand; the first two 16-byte chunks are all
-// the region-I path reads.  lo / hi: the grid indices [lo, hi] of the chunk
-// where the line's |x| + y < 15 (W4 regions II-IV; empty: lo > hi); step two
-// leaves those pairs to the core pass.
-struct __align__(16) CondPairX {
-    float Cy[2], D2[2];
-    float Pc[2];
-    int lo[2];
-    int hi[2];
-    int pad[2];
+// Region-I constants of a line for the C conditions of its group, each
+// array in condition order: conditions 2k and 2k+1 are one packed FP32x2
+// operand, conditions 4k..4k+3 one 16-byte load.  This is all step two
+// stages per (line, group) besides LineShX: 12 bytes per condition (C = 2 is
+// padded to 32 bytes, a whole number of 16-byte copies).
+template <int C>
+struct __align__(16) LineR1 {
+    float Cy[C], D2[C], Pc[C];
 };
-static_assert(sizeof(CondPairX) == 48, "CondPairX layout");
+template <>
+struct __align__(16) LineR1<2> {
+    float Cy[2], D2[2], Pc[2], pad[2];
+};
+static_assert(sizeof(LineR1<8>) == 96 && sizeof(LineR1<4>) == 48 && sizeof(LineR1<2>) == 32,
+              "LineR1 layout");
+// The grid indices [lo, hi] of the chunk where the line's |x| + y < 15 (W4
+// regions II-IV; empty: lo > hi), per condition of the group: step two
+// leaves those pairs to the core pass.  Read from memory (not staged) by the
+// core-candidate lines only.
+template <int C>
+struct __align__(16) LineIv {
+    int lo[C], hi[C];
+};
+// Bytes per (line, group) of the mixed multi-condition region-I records.
+constexpr size_t line_r1_bytes(int C) { return C == 8 ? 96 : (C == 4 ? 48 : 32); }
 // Per (line, condition) of the mixed multi-condition layout, for the core
 // pass: the grid indices of W4 regions II-IV [lo15, hi15] and III-IV
 // [lo55, hi55] (empty: lo > hi) inside the line's window.
@@ -200,6 +212,7 @@ struct PrepArgs {
                         // (LineShX mixed, LineSh64 FP64)
     CoreIv* civ;        // mixed multi-condition: region intervals and
     float2* cyp;        //   (y, pref) per (condition, line), condition-major
+    int* liv;           // mixed multi-condition: LineIv<group> per (line, group)
     // Temperature class of each condition: conditions of one class have the
     // same beta, Q, T_ref/T and Doppler width, so their intensity, Lorentz
     // temperature power and 1/Doppler width are the same numbers.
@@ -217,6 +230,7 @@ struct StepArgs {
     size_t out_stride;  // elements between conditions
     GridDev G;
     const void* lsh;    // multi-condition layout (LineShX mixed, LineSh64 FP64)
+    const int* liv;     // mixed multi-condition: LineIv<group> per (line, group)
     int group;          // conditions per group (multi-condition kernel)
     int tiles_per_cond;
     int n_items;
@@ -253,7 +267,7 @@ size_t record_bytes(int kind, bool mixed);
 // `ncond` conditions of `n` lines, the per-line grid index and the
 // per-condition core widths; sections 256-byte aligned from `base_off`.
 struct ScratchPlan {
-    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, need;
+    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, off_liv, need;
 };
 ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off,
                          int group = 0);

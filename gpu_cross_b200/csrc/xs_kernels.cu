@@ -181,11 +181,10 @@ __device__ __forceinline__ void region_interval_q(double nu, double g, double y,
 
 // `reach` (mixed Voigt): the largest distance, in grid points, from the
 // line's nearest grid index to its region interval (the core pass's reach).
-// `pair`: the mixed-precision multi-condition layout fills its condition's
-// half of a CondPairX there (k_prep_pairs stores the whole record).
+// The mixed-precision multi-condition layout has its own step one
+// (k_prep_group_x); the FP64 one is written here.
 template <int KIND, int CONV, bool MIXED>
-__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondPairX* pair = nullptr,
-                                         int* reach = nullptr) {
+__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* reach = nullptr) {
     const CondDev& C = a.cond[c];
     const double* F = a.G.freq;
     const double f0 = F[0];
@@ -295,8 +294,9 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
             kcl = w < 3.0e7 ? int(w) : 30000000;
         }
         if (c == 0) a.mi[i] = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
-        if (a.group > 0) {
-            // Multi-condition layout (conditions of a group share the window).
+        if (!MIXED && a.group > 0) {
+            // FP64 multi-condition layout (conditions of a group share the
+            // window).
             const int C = a.group;
             const int cg = c / C, cl = c - cg * C;
             const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(i);
@@ -308,51 +308,7 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
                 const int bb = int(fmin(chi_d - m, 32767.0));
                 core = aa | (bb << 16);
             }
-            if (MIXED) {
-                // Region intervals: the grid indices of the line's window
-                // where |x| + y < 15 (W4 regions II-IV) and < 5.5 (III-IV),
-                // with x = (nu - f_j) g in FP64 on the analytic grid
-                // f_j = f0 + j df, so that the region of every pair is the
-                // FP64 choice (up to the grid's last-bit rounding) and never
-                // flips with the FP32 rounding of x.  Step two leaves the
-                // pairs of [lo15, hi15] to the core pass.
-                const bool far_m = !(fabs(m) < 16000000.0);
-                CoreIv iv;
-                region_interval(nu_p, g, y, 15.0, lo, hi, f0, df, iv.lo15, iv.hi15);
-                region_interval(nu_p, g, y, 5.5, lo, hi, f0, df, iv.lo55, iv.hi55);
-                int rch = 0;
-                if (iv.lo15 <= iv.hi15) {
-                    const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
-                    rch = w < 3.0e7 ? int(w) : 30000000;
-                    if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
-                }
-                if (reach) *reach = rch;
-                // a whole line is a core candidate of every tile
-                kcl = whole ? 30000000 : rch;
-                const size_t ci2 = size_t(c) * size_t(a.L.n) + size_t(i);
-                a.civ[ci2] = iv;
-                a.cyp[ci2] = make_float2(float(y), float(pref));
-                // conditions 2k, 2k+1 share one CondPairX
-                CondPairX& cp = *pair;
-                const int h = c & 1;  // groups have an even size
-                cp.Cy[h] = float(Cy);
-                cp.D2[h] = float(D2);
-                cp.Pc[h] = float(Pc);
-                cp.lo[h] = iv.lo15;
-                cp.hi[h] = iv.hi15;
-                cp.pad[h] = 0;
-                if (cl == 0) {
-                    LineShX ls;
-                    ls.m = float(far_m ? 0.0 : m);
-                    ls.dfn = float(df / nu_p);
-                    ls.rn = float(((nu_p - f0) - m * df) / nu_p);
-                    ls.whole = far_m ? 1 : 0;
-                    ls.lo = lo;
-                    ls.hi = hi;
-                    ls.nu = nu_p;
-                    reinterpret_cast<LineShX*>(a.lsh)[gi] = ls;
-                }
-            } else {
+            {
                 CondRec64 cr;
                 cr.g = g;
                 cr.Cy = Cy;
@@ -458,53 +414,12 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, CondP
     return kcl;
 }
 
-// Step one of the mixed-precision multi-condition layout: one thread per
-// (line, pair of conditions), so that each CondPairX is stored whole.
-template <int CONV>
-__global__ void __launch_bounds__(256) k_prep_pairs(PrepArgs a) {
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int c0 = 2 * int(blockIdx.y);
-    int k0 = 0, k1 = 0, r0 = 0, r1 = 0;
-    if (i < a.L.n) {
-        CondPairX cp;
-        k0 = prep_line<kVoigt, CONV, true>(a, i, c0, &cp, &r0);
-        k1 = prep_line<kVoigt, CONV, true>(a, i, c0 + 1, &cp, &r1);
-        const int C = a.group;
-        const int cg = c0 / C;
-        const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(i);
-        float4* dst = reinterpret_cast<float4*>(reinterpret_cast<CondPairX*>(a.rec) + gi * (C / 2) + (c0 - cg * C) / 2);
-        const float4* src = reinterpret_cast<const float4*>(&cp);
-#pragma unroll
-        for (int q = 0; q < int(sizeof(CondPairX) / 16); ++q) dst[q] = src[q];
-    }
-    // block maxima of the core-candidate widths (kc) and of the core pass's
-    // reach (kc + kMaxCond), one atomic each per block
-    __shared__ int smax[4][8];
-    k0 = __reduce_max_sync(0xffffffffu, k0);
-    k1 = __reduce_max_sync(0xffffffffu, k1);
-    r0 = __reduce_max_sync(0xffffffffu, r0);
-    r1 = __reduce_max_sync(0xffffffffu, r1);
-    if ((threadIdx.x & 31) == 0) {
-        smax[0][threadIdx.x >> 5] = k0;
-        smax[1][threadIdx.x >> 5] = k1;
-        smax[2][threadIdx.x >> 5] = r0;
-        smax[3][threadIdx.x >> 5] = r1;
-    }
-    __syncthreads();
-    if (threadIdx.x < 4) {
-        int m = 0;
-        for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[threadIdx.x][w] > m ? smax[threadIdx.x][w] : m;
-        const int slot = (threadIdx.x >= 2 ? kMaxCond : 0) + c0 + int(threadIdx.x & 1);
-        if (m > 0) atomicMax(a.kc + slot, m);
-    }
-}
-
 template <int KIND, int CONV, bool MIXED>
 __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
     int kcl = 0, rch = 0;
-    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, nullptr, &rch);
+    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, &rch);
     if (KIND == kVoigt) {
         // Block maxima of the core widths (kc) and, mixed, of the core pass's
         // reach (kc + kMaxCond), one atomic each per block.
@@ -530,17 +445,15 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
 // the condition-free offsets (LineShX) -- is computed once; the C conditions
 // follow in order, and a condition of the same temperature class as the one
 // before it (same beta, Q, T_ref/T and Doppler width, set by the host) reuses
-// its intensity, Lorentz temperature power and 1/Doppler width.  The
-// arithmetic of every value is prep_line's (same operations in the same
-// order), so the records are the same bits.  A line's C/2 CondPairX of the
-// group are contiguous and stored one after the other by the same thread,
-// so each warp fills whole sectors of its records.  Blocks are numbered group
-// fastest: the groups of one range of lines run side by side and share its
-// line data in L2.
+// its intensity, Lorentz temperature power and 1/Doppler width.  Each value
+// takes the FP64 path's operations in the same order (the W4 region
+// intervals are the FP64 region choice).  A line's records of the group
+// (LineR1, LineIv) are contiguous and stored whole by one thread, so each
+// warp fills whole sectors.  Blocks are numbered group fastest: the groups
+// of one range of lines run side by side and share its line data in L2.
 template <int CONV, int C>
 __global__ void __launch_bounds__(128, 4) k_prep_group_x(PrepArgs a) {
     static_assert(C % 2 == 0, "conditions come in pairs");
-    constexpr int NP = C / 2;
     const int ngroups = a.ncond / C;
     const long blk = long(blockIdx.x);
     const int cg = int(blk % ngroups);
@@ -605,7 +518,8 @@ __global__ void __launch_bounds__(128, 4) k_prep_group_x(PrepArgs a) {
 
     double S = 0.0, pw = 0.0, g = 0.0;
     int prev_class = -1;
-    CondPairX cp;
+    LineR1<C> lr;
+    LineIv<C> li;
 #pragma unroll
     for (int k = 0; k < C; ++k) {
         const int c = cg * C + k;
@@ -642,19 +556,11 @@ __global__ void __launch_bounds__(128, 4) k_prep_group_x(PrepArgs a) {
             const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
             a.civ[ci] = iv;
             a.cyp[ci] = make_float2(float(y), float(pref));
-            const int h = k & 1;
-            cp.Cy[h] = float(y2 - 0.5);
-            cp.D2[h] = float(2.0 * y2);
-            cp.Pc[h] = float(Pc);
-            cp.lo[h] = iv.lo15;
-            cp.hi[h] = iv.hi15;
-            cp.pad[h] = 0;
-            if (h == 1) {
-                float4* dst = reinterpret_cast<float4*>(reinterpret_cast<CondPairX*>(a.rec) + gi * NP + k / 2);
-                const float4* src = reinterpret_cast<const float4*>(&cp);
-#pragma unroll
-                for (int q = 0; q < int(sizeof(CondPairX) / 16); ++q) dst[q] = src[q];
-            }
+            lr.Cy[k] = float(y2 - 0.5);
+            lr.D2[k] = float(2.0 * y2);
+            lr.Pc[k] = float(Pc);
+            li.lo[k] = iv.lo15;
+            li.hi[k] = iv.hi15;
         }
         kcl = __reduce_max_sync(0xffffffffu, kcl);
         rch = __reduce_max_sync(0xffffffffu, rch);
@@ -662,6 +568,20 @@ __global__ void __launch_bounds__(128, 4) k_prep_group_x(PrepArgs a) {
             smax[0][k][warp] = kcl;
             smax[1][k][warp] = rch;
         }
+    }
+    if (live) {
+        // the line's records of the group, stored whole (16-byte stores)
+        if constexpr (C == 2) {
+            lr.pad[0] = lr.pad[1] = 0.0f;
+        }
+        float4* dst = reinterpret_cast<float4*>(reinterpret_cast<LineR1<C>*>(a.rec) + gi);
+        const float4* src = reinterpret_cast<const float4*>(&lr);
+#pragma unroll
+        for (int q = 0; q < int(sizeof(LineR1<C>) / 16); ++q) dst[q] = src[q];
+        int4* idst = reinterpret_cast<int4*>(reinterpret_cast<LineIv<C>*>(a.liv) + gi);
+        const int4* isrc = reinterpret_cast<const int4*>(&li);
+#pragma unroll
+        for (int q = 0; q < int(sizeof(LineIv<C>) / 16); ++q) idst[q] = isrc[q];
     }
     // block maxima of the core-candidate widths (kc) and of the core pass's
     // reach (kc + kMaxCond), one atomic each per block and condition
@@ -1567,9 +1487,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt_mc(StepArgs a) {
 // and about three issue slots in all.  The pairs inside a line's region
 // interval (|x| + y < 15, from step one) are left to k_core_mcx.
 // ---------------------------------------------------------------------------
+// Resident blocks per SM the mixed multi-condition kernel asks the compiler
+// to fit: 24 warps per SM (about 80 registers a thread), except 8 conditions
+// at 8 warps per block, which keeps 124 registers and 16 warps per SM -- the
+// two occupancy points the autotuner chooses between through the block size.
 template <int C, int WARPS>
 constexpr int voigt_mcx_min_blocks() {
-    return C <= 2 ? 24 / WARPS : (C == 4 ? 20 / WARPS : 16 / WARPS);
+    return (C == 8 && WARPS == 8) ? 2 : 24 / WARPS;
 }
 
 template <int C, int WARPS>
@@ -1580,9 +1504,9 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    using R1 = LineR1<C>;
     LineShX* lsb = reinterpret_cast<LineShX*>(smem_raw) + warp * 64;
-    CondPairX* cpb = reinterpret_cast<CondPairX*>(smem_raw + size_t(WARPS) * 64 * sizeof(LineShX)) +
-                     warp * 64 * NP;
+    R1* rb = reinterpret_cast<R1*>(smem_raw + size_t(WARPS) * 64 * sizeof(LineShX)) + warp * 64;
 
     for (;;) {
         int item = 0;
@@ -1613,16 +1537,13 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         const int E = int(warp_lower_bound(La, Lb, lane, [&](long i) { return mi[i] >= t0 - kc; }));
         const int Fc = int(warp_lower_bound(E, Lb, lane, [&](long i) { return mi[i] > tl + kc; }));
         const LineShX* lsh = reinterpret_cast<const LineShX*>(a.lsh) + gbase;
-        const CondPairX* cpr = reinterpret_cast<const CondPairX*>(a.rec) + gbase * NP;
+        const R1* r1 = reinterpret_cast<const R1*>(a.rec) + gbase;
+        const LineIv<C>* ivl = reinterpret_cast<const LineIv<C>*>(a.liv) + gbase;
 
         const int jj = t0 + lane;
         const float jf = float(jj);
-        const double fj = a.G.freq[jj < t1 ? jj : tl];
-        float kx[C];
         float2 k2[NP];
         float2 acc[NP], sum[NP], cmp[NP];
-#pragma unroll
-        for (int c = 0; c < C; ++c) kx[c] = a.kx[cg * C + c];
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
             k2[p] = f2(a.kx2[cg * C + 2 * p], a.kx2[cg * C + 2 * p + 1]);
@@ -1635,11 +1556,12 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         // mask, so that an infinite reciprocal of a skipped pair never
         // reaches the sum); with GUARD the product itself is selected, for
         // lines whose u may overflow.
-        auto region1 = [&](auto guard, float X2, const CondPairX& r, int p, bool keep0, bool keep1) {
-            const float4 f0 = *reinterpret_cast<const float4*>(&r.Cy[0]);
-            const float2 pc = *reinterpret_cast<const float2*>(&r.Pc[0]);
-            const float2 u = __ffma2_rn(f2(X2, X2), k2[p], f2(f0.x, f0.y));
-            const float2 den = __ffma2_rn(u, u, f2(f0.z, f0.w));
+        auto region1 = [&](auto guard, float X2, const R1& r, int p, bool keep0, bool keep1) {
+            const float2 cy = *reinterpret_cast<const float2*>(&r.Cy[2 * p]);
+            const float2 d2 = *reinterpret_cast<const float2*>(&r.D2[2 * p]);
+            const float2 pc = *reinterpret_cast<const float2*>(&r.Pc[2 * p]);
+            const float2 u = __ffma2_rn(f2(X2, X2), k2[p], cy);
+            const float2 den = __ffma2_rn(u, u, d2);
             const float2 num = __ffma2_rn(u, pc, pc);
             const float2 rr = f2(keep0 ? rcp_approx_f32(den.x) : 0.0f, keep1 ? rcp_approx_f32(den.y) : 0.0f);
             if constexpr (decltype(guard)::value) {
@@ -1657,31 +1579,31 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         // (kPairTau: every scaled value stays a normal FP32 number for the
         // region-I pairs of lines that are not whole).  Pairs where `keep`
         // is false add exactly zero.
-        auto region1_ab = [&](float X2, const CondPairX& rA, const CondPairX& rB, int pA, int pB,
-                              bool keep) {
-            const float4 fA = *reinterpret_cast<const float4*>(&rA.Cy[0]);
-            const float4 fB = *reinterpret_cast<const float4*>(&rB.Cy[0]);
-            const float2 pcA = *reinterpret_cast<const float2*>(&rA.Pc[0]);
-            const float2 pcB = *reinterpret_cast<const float2*>(&rB.Pc[0]);
-            const float2 uA = __ffma2_rn(f2(X2, X2), k2[pA], f2(fA.x, fA.y));
-            const float2 uB = __ffma2_rn(f2(X2, X2), k2[pB], f2(fB.x, fB.y));
-            const float2 dA = __ffma2_rn(uA, uA, f2(fA.z, fA.w));
-            const float2 dB = __ffma2_rn(uB, uB, f2(fB.z, fB.w));
-            const float2 nA = __ffma2_rn(uA, pcA, pcA);
-            const float2 nB = __ffma2_rn(uB, pcB, pcB);
+        // pA = 2q, pB = 2q + 1: conditions 4q..4q+3, one 16-byte load for
+        // each of Cy, D2 and Pc.
+        auto region1_ab = [&](float X2, const R1& r, int pA, int pB, bool keep) {
+            const float4 cy = *reinterpret_cast<const float4*>(&r.Cy[2 * pA]);
+            const float4 d2 = *reinterpret_cast<const float4*>(&r.D2[2 * pA]);
+            const float4 pc = *reinterpret_cast<const float4*>(&r.Pc[2 * pA]);
+            const float2 uA = __ffma2_rn(f2(X2, X2), k2[pA], f2(cy.x, cy.y));
+            const float2 uB = __ffma2_rn(f2(X2, X2), k2[pB], f2(cy.z, cy.w));
+            const float2 dA = __ffma2_rn(uA, uA, f2(d2.x, d2.y));
+            const float2 dB = __ffma2_rn(uB, uB, f2(d2.z, d2.w));
+            const float2 nA = __ffma2_rn(uA, f2(pc.x, pc.y), f2(pc.x, pc.y));
+            const float2 nB = __ffma2_rn(uB, f2(pc.z, pc.w), f2(pc.z, pc.w));
             const float2 aA = __fmul2_rn(dA, f2s(kPairTau));
             const float2 bB = __fmul2_rn(dB, f2s(kPairTau));
             const float2 q = __fmul2_rn(aA, dB);
-            const float2 r = keep ? f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)) : f2(0.0f, 0.0f);
-            acc[pA] = __ffma2_rn(nA, __fmul2_rn(bB, r), acc[pA]);
-            acc[pB] = __ffma2_rn(nB, __fmul2_rn(aA, r), acc[pB]);
+            const float2 rq = keep ? f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)) : f2(0.0f, 0.0f);
+            acc[pA] = __ffma2_rn(nA, __fmul2_rn(bB, rq), acc[pA]);
+            acc[pB] = __ffma2_rn(nB, __fmul2_rn(aA, rq), acc[pB]);
         };
 
         const int ngroups = split_groups(Lb - La, a.splits, split);
         auto gstart = [&](int gi) { return La + 32 * (split + gi * a.splits); };
         auto stage_group = [&](int bufi, int b, int cnt) {
             stage(lsb + bufi * 32, lsh + b, cnt, lane);
-            stage(cpb + bufi * 32 * NP, cpr + size_t(b) * NP, cnt * NP, lane);
+            stage(rb + bufi * 32, r1 + b, cnt, lane);
         };
         if (ngroups > 0) {
             const int b = gstart(0);
@@ -1700,7 +1622,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             }
             __syncwarp();
             const LineShX* SL = lsb + (gi & 1) * 32;
-            const CondPairX* SC = cpb + (gi & 1) * 32 * NP;
+            const R1* SR = rb + (gi & 1) * 32;
             const int gb = gstart(gi);
             const int ge = Lb - gb < 32 ? Lb : gb + 32;
             auto lo_of = [&](int v) { return (v < gb ? gb : (v > ge ? ge : v)) - gb; };
@@ -1715,11 +1637,10 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     const float X2 = X * X;
                     if constexpr (NP % 2 == 0) {
 #pragma unroll
-                        for (int p = 0; p < NP; p += 2)
-                            region1_ab(X2, SC[t * NP + p], SC[t * NP + p + 1], p, p + 1, true);
+                        for (int p = 0; p < NP; p += 2) region1_ab(X2, SR[t], p, p + 1, true);
                     } else {
 #pragma unroll
-                        for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, true, true);
+                        for (int p = 0; p < NP; ++p) region1(plain, X2, SR[t], p, true, true);
                     }
                 }
             };
@@ -1732,11 +1653,10 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     const float X2 = X * X;
                     if constexpr (NP % 2 == 0) {
 #pragma unroll
-                        for (int p = 0; p < NP; p += 2)
-                            region1_ab(X2, SC[t * NP + p], SC[t * NP + p + 1], p, p + 1, in);
+                        for (int p = 0; p < NP; p += 2) region1_ab(X2, SR[t], p, p + 1, in);
                     } else {
 #pragma unroll
-                        for (int p = 0; p < NP; ++p) region1(plain, X2, SC[t * NP + p], p, in, in);
+                        for (int p = 0; p < NP; ++p) region1(plain, X2, SR[t], p, in, in);
                     }
                 }
             };
@@ -1746,19 +1666,25 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     const LineShX s = SL[t];
                     const bool full = (t >= a1 && t < d1);
                     const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
-                    const float X = s.whole ? float((s.nu - fj) / s.nu) : fmaf(s.m - jf, s.dfn, s.rn);
+                    // whole lines: X from the FP64 centre (rare; the grid
+                    // value is read here rather than held for every line)
+                    const float X = s.whole ? float((s.nu - a.G.freq[jj < t1 ? jj : tl]) / s.nu)
+                                            : fmaf(s.m - jf, s.dfn, s.rn);
                     const float X2 = X * X;
                     const float aX = fabsf(X);
+                    const LineIv<C> iv = ivl[gb + t];  // the conditions' core intervals
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
-                        const CondPairX& r = SC[t * NP + p];
                         bool keep[2];
 #pragma unroll
-                        for (int h = 0; h < 2; ++h)
+                        for (int h = 0; h < 2; ++h) {
+                            const int c = 2 * p + h;
                             // beyond x ~ 1e9 (lines far off the FP32 offset
                             // range) region I is taken as 0
-                            keep[h] = in && !(jj >= r.lo[h] && jj <= r.hi[h]) && aX * kx[2 * p + h] < 1.0e9f;
-                        region1(guarded, X2, r, p, keep[0], keep[1]);
+                            keep[h] = in && !(jj >= iv.lo[c] && jj <= iv.hi[c]) &&
+                                      aX * a.kx[cg * C + c] < 1.0e9f;
+                        }
+                        region1(guarded, X2, SR[t], p, keep[0], keep[1]);
                     }
                 }
             };
@@ -2196,7 +2122,7 @@ cudaError_t run_voigt_mc(int blocks, const StepArgs& a, cudaStream_t st, int* oc
 
 template <int C, int WARPS>
 cudaError_t run_voigt_mcx(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
-    const size_t smem = size_t(WARPS) * 64 * (sizeof(LineShX) + (C / 2) * sizeof(CondPairX));
+    const size_t smem = size_t(WARPS) * 64 * (sizeof(LineShX) + sizeof(LineR1<C>));
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(k_steptwo_voigt_mcx<C, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)) != cudaSuccess)
@@ -2327,7 +2253,9 @@ cudaError_t launch_reduce_splits(const StepArgs& a, int ncond_out, cudaStream_t 
 cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaStream_t stream) {
     if (a.L.n <= 0 || a.ncond <= 0) return cudaSuccess;
     const dim3 grid(unsigned((a.L.n + 255) / 256), unsigned(a.ncond));
-    if (kind == kVoigt && mixed && a.group > 0 && a.L.s32 == nullptr) {
+    if (kind == kVoigt && mixed && a.group > 0) {
+        // (precomputed-intensity lists run one condition at a time)
+        if (a.L.s32 != nullptr) return cudaErrorInvalidValue;
         // one thread per (line, group), group fastest
         const long ngroups = a.ncond / a.group;
         const long nblk = (a.L.n + 127) / 128 * ngroups;
@@ -2349,10 +2277,6 @@ cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaS
             default:
                 return cudaErrorInvalidValue;
         }
-    } else if (kind == kVoigt && mixed && a.group > 0) {
-        const dim3 pgrid(grid.x, unsigned(a.ncond / 2));
-        if (conv == kConvGpu) k_prep_pairs<kConvGpu><<<pgrid, 256, 0, stream>>>(a);
-        else k_prep_pairs<kConvCpu><<<pgrid, 256, 0, stream>>>(a);
     } else if (kind == kVoigt) {
         if (conv == kConvGpu) {
             if (mixed) k_prep<kVoigt, kConvGpu, true><<<grid, 256, 0, stream>>>(a);
@@ -2425,11 +2349,14 @@ size_t record_bytes(int kind, bool mixed) {
 ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off, int group) {
     auto al = [](size_t v) { return (v + 255) / 256 * 256; };
     ScratchPlan p;
-    const size_t rec = group > 0 ? (mixed ? sizeof(CondPairX) / 2 : sizeof(CondRec64))
-                                 : record_bytes(kind, mixed);
     const size_t nwin = group > 0 ? size_t((ncond + group - 1) / group) : size_t(ncond);
+    // records: per (line, condition), or for the mixed multi-condition layout
+    // one LineR1<group> per (line, group)
+    const size_t rec_bytes = group > 0 ? (mixed ? line_r1_bytes(group) * n * nwin
+                                                : sizeof(CondRec64) * n * size_t(ncond))
+                                       : record_bytes(kind, mixed) * n * size_t(ncond);
     p.off_rec = al(base_off);
-    p.off_wlo = al(p.off_rec + rec * n * size_t(ncond));
+    p.off_wlo = al(p.off_rec + rec_bytes);
     p.off_whi = al(p.off_wlo + sizeof(int) * n * nwin);
     p.off_mi = al(p.off_whi + sizeof(int) * n * nwin);
     p.off_kc = al(p.off_mi + sizeof(int) * n);
@@ -2438,7 +2365,8 @@ ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_
     p.off_civ = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
     const bool core = mixed && group > 0;
     p.off_cyp = al(p.off_civ + (core ? sizeof(CoreIv) * n * size_t(ncond) : 0));
-    p.need = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
+    p.off_liv = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
+    p.need = al(p.off_liv + (core ? 2 * sizeof(int) * size_t(group) * n * nwin : 0));
     return p;
 }
 
