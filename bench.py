@@ -41,6 +41,27 @@ if ROOT not in sys.path:
 # rational's numerator and denominator, the scale and the accumulate, with the
 # per-line terms hoisted (the reciprocal runs on the XU pipe, not counted)
 FLOPS_PER_PAIR = 14
+# XU-pipe reciprocals per region-I pair: two pairs of line-evals share one
+RCP_PER_PAIR = 0.5
+
+
+def hbm_view(traffic_bytes, ms):
+    """Step two's DRAM traffic per launch over its time, against the
+    measured copy bandwidth of this pool's B200s (MEASURED_PEAKS.json)."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = None
+    if os.path.exists(path):
+        try:
+            peak = float(json.load(open(path))["hbm_gbs"])
+        except (OSError, ValueError, KeyError):
+            peak = None
+    if not traffic_bytes or not ms:
+        return {"peak_gbs": peak, "achieved_gbs": None, "frac": None}
+    gbs = traffic_bytes / (ms * 1e-3) / 1e9
+    return {"peak_gbs": peak, "achieved_gbs": gbs, "frac": gbs / peak if peak else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peak else None}
+
+
 METRIC = "Voigt line-evals/s & p99 request latency: mixed-precision batched vs plain FP64"
 
 
@@ -593,6 +614,12 @@ def run_ours(args, rank, world, dist):
             "other_peaks": peaks,
             "region_share": regions,
             "xu_pipe_pct_ncu": xu_pct if args.workload == "sweep" else None,
+            "mufu_view": {
+                "achieved_rcp_per_s": pairs_step * RCP_PER_PAIR / (step2_ms * 1e-3),
+                "peak_rcp_per_s": peaks.get("rcp32_tops", 0.0) * 1e12,
+                "rcp_per_pair": RCP_PER_PAIR,
+                "note": "reciprocals on the XU pipe: one per two region-I line-evals (shared)"},
+            "hbm_view": hbm_view(traffic, step2_ms),
         },
         "cpu_baseline": cpu,
         "reference_gpu_kernel": ref_gpu,
