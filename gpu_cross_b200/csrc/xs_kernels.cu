@@ -720,6 +720,12 @@ __device__ __forceinline__ fcplx operator*(fcplx a, fcplx b) {
 //   Re[T N / D] = y [(a + b y^2 - 3 b x^2) Dr + 2 x^2 (3 + 2 Ur)(Nr + 2 b y^2)] / |D|^2
 // (expanding Re[T N conj(D)]); a complex evaluation would cancel by a factor
 // x / y in the wings of narrow lines.
+// a / b for the FP32 W4 forms of regions II and III (no cancellation
+// follows there): the hardware reciprocal and one product, within 2 ulp; the
+// denominators lie between about 0.5 and 1e6, far from the range where the
+// approximation fails.  Region IV, which subtracts, keeps the IEEE division.
+__device__ __forceinline__ float region_div(float a, float b) { return __fdividef(a, b); }
+
 template <class R>
 __device__ __forceinline__ R w4_region2_re(R x, R y) {
     const R a = R(1.410474), b = R(.5641896), c = R(.75);
@@ -729,7 +735,7 @@ __device__ __forceinline__ R w4_region2_re(R x, R y) {
     const R dr = c + R(3) * ur + ur * ur - ui * ui;
     const R di = ui * (R(3) + R(2) * ur);
     const R br = (a + b * y2 - R(3) * b * x2) * dr + R(2) * x2 * (R(3) + R(2) * ur) * (nr + R(2) * b * y2);
-    return y * br / (dr * dr + di * di);
+    return region_div(y * br, dr * dr + di * di);
 }
 
 // W4 region III in FP32 (there y >= 0.195|x| - 0.176, so Re w is not small
@@ -738,7 +744,7 @@ __device__ __forceinline__ float w4_region3_re_f32(float x, float y) {
     const fcplx t = {y, -x};
     const fcplx num = 16.4955f + t * (20.20933f + t * (11.96482f + t * (3.778987f + t * fcplx{.5642236f, 0.f})));
     const fcplx den = 16.4955f + t * (38.82363f + t * (39.27121f + t * (21.69274f + t * (6.699398f + t))));
-    return (num.re * den.re + num.im * den.im) / (den.re * den.re + den.im * den.im);
+    return region_div(num.re * den.re + num.im * den.im, den.re * den.re + den.im * den.im);
 }
 
 // a - u p for the region IV Horner schemes.
