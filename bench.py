@@ -509,8 +509,13 @@ def run_ours(args, rank, world, dist):
     # error statement of the mixed result: the a-priori bound and a sampled
     # FP64 re-evaluation of 8 rows per condition (one execute outside the
     # timed region)
+    shape = (tuned or {}).get("mixed") or {}
     o_chk = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=capi.MIXED,
-                              ref_temp=common["ref_temp"], check_rows=8)
+                              ref_temp=common["ref_temp"],
+                              points_per_thread=shape.get("points_per_thread", args.P),
+                              warps_per_block=shape.get("warps_per_block", args.W),
+                              conditions_per_warp=shape.get("conditions_per_warp", args.C),
+                              line_splits=args.S, check_rows=8)  # the timed launch shape
     out.zero_()
     eng.execute(o_chk, cc, L, G, out.data_ptr(), npts)
     error_statement = eng.accuracy()

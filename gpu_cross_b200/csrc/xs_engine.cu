@@ -603,17 +603,22 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
                 pa.cond[c].beta = ov->beta;
             }
         }
-        // temperature classes: the first condition with the same constants
+        // temperature classes, numbered in order of first appearance
+        pa.nclass = 0;
         for (int c = 0; c < nc; ++c) {
-            pa.tclass[c] = c;
-            for (int k = 0; k < c; ++k) {
+            pa.tclass[c] = -1;
+            for (int t = 0; t < pa.nclass; ++t) {
                 const CondDev& x = pa.cond[c];
-                const CondDev& y = pa.cond[k];
+                const CondDev& y = pa.cond[pa.class_rep[t]];
                 if (x.cmcoef == y.cmcoef && x.beta == y.beta && x.partition == y.partition &&
                     x.tratio == y.tratio && x.dpw == y.dpw) {
-                    pa.tclass[c] = pa.tclass[k];
+                    pa.tclass[c] = t;
                     break;
                 }
+            }
+            if (pa.tclass[c] < 0) {
+                pa.tclass[c] = pa.nclass;
+                pa.class_rep[pa.nclass++] = c;
             }
         }
         pa.rec = base + plan.off_rec;

@@ -213,11 +213,17 @@ struct PrepArgs {
     CoreIv* civ;        // mixed multi-condition: region intervals and
     float2* cyp;        //   (y, pref) per (condition, line), condition-major
     int* liv;           // mixed multi-condition: LineIv<group> per (line, group)
-    // Temperature class of each condition: conditions of one class have the
-    // same beta, Q, T_ref/T and Doppler width, so their intensity, Lorentz
-    // temperature power and 1/Doppler width are the same numbers.
+    // Temperature classes: conditions of one class have the same cmcoef,
+    // beta, Q, T_ref/T and Doppler width, so their intensity, Lorentz
+    // temperature power and 1/Doppler width are the same numbers.  tclass[c]
+    // in [0, nclass); class_rep[t]: a condition of class t.
+    int nclass;
     int tclass[kMaxCond];
+    int class_rep[kMaxCond];
 };
+// Temperature classes whose per-line values step one keeps in shared memory
+// (more classes: each condition computes its own).
+constexpr int kMaxClassCache = 16;
 
 struct StepArgs {
     const void* rec;

@@ -439,27 +439,27 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
     }
 }
 
-// Step one of the mixed-precision multi-condition layout, one thread per
-// (line, group of C conditions).  The line's data is read once per group;
-// what the group's conditions share -- the window, the nearest grid index,
-// the condition-free offsets (LineShX) -- is computed once; the C conditions
-// follow in order, and a condition of the same temperature class as the one
-// before it (same beta, Q, T_ref/T and Doppler width, set by the host) reuses
-// its intensity, Lorentz temperature power and 1/Doppler width.  Each value
-// takes the FP64 path's operations in the same order (the W4 region
-// intervals are the FP64 region choice).  A line's records of the group
-// (LineR1, LineIv) are contiguous and stored whole by one thread, so each
-// warp fills whole sectors.  Blocks are numbered group fastest: the groups
-// of one range of lines run side by side and share its line data in L2.
+// Step one of the mixed-precision multi-condition layout, one thread per line
+// over every group of C conditions.  The line's data is read once; the
+// intensity, the Lorentz temperature power and 1/Doppler width of each
+// temperature class (conditions with the same beta, Q, T_ref/T and Doppler
+// width; the 40-condition sweep has 10) are computed once per line and kept
+// in shared memory (up to kMaxClassCache classes; beyond, each condition
+// computes its own); what a group's conditions share -- the window, the
+// condition-free offsets (LineShX) -- is written per group; the conditions
+// follow in order, their loop not unrolled, which keeps the code small.
+// Each value takes the FP64 path's operations in the same order (the W4
+// region intervals are the FP64 region choice).  A line's records of a
+// group (LineR1, LineIv) are contiguous and written by one thread within a
+// short time, so whole sectors reach memory.
 template <int CONV, int C>
-__global__ void __launch_bounds__(128, 4) k_prep_group_x(PrepArgs a) {
+__global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
     static_assert(C % 2 == 0, "conditions come in pairs");
+    extern __shared__ __align__(16) double cls[];  // [3][ncache][256]: S, (T_ref/T)^n, g
+    __shared__ int smax[2][kMaxCond][8];
     const int ngroups = a.ncond / C;
-    const long blk = long(blockIdx.x);
-    const int cg = int(blk % ngroups);
-    const long i = (blk / ngroups) * 128 + threadIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __shared__ int smax[2][C][4];
+    const long i = long(blockIdx.x) * 256 + threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool live = i < a.L.n;
     const double* F = a.G.freq;
     const double f0 = F[0];
@@ -469,129 +469,135 @@ __global__ void __launch_bounds__(128, 4) k_prep_group_x(PrepArgs a) {
     double nu = 0.0, ei = 0.0, aif = 0.0, gns = 0.0, gam = 0.0, nex = 0.0;
     if (live) {
         nu = a.L.nu[i];
-        if (cg == 0 && i > 0 && nu < a.L.nu[i - 1]) atomicOr(a.err, kErrUnsorted);
+        if (i > 0 && nu < a.L.nu[i - 1]) atomicOr(a.err, kErrUnsorted);
         ei = a.L.energies[i];
         aif = a.L.aif[i];
         gns = double(a.L.gns[i]);
         gam = a.L.gamma[i];
         nex = a.L.nexp[i];
     }
-    const double cut = a.cond[cg * C].cut;  // a group shares its cut
     double nu_if = nu;
     if (nu_if == 0) nu_if = 1e-6;
-    double nu_p;
-    int lo = s, hi = s;
-    if (CONV == kConvGpu) {
-        nu_p = nu;  // step two reads the uploaded centre (cross_kernal.cu:951)
-        if (live) {
-            // -cut <= nu - f <= cut (cross_kernal.cu:952-957)
-            lo = find_first(s, e, ceil((nu - cut - f0) / df), [&](int j) { return !(nu - F[j] > cut); });
-            hi = find_first(s, e, ceil((nu + cut - f0) / df), [&](int j) { return nu - F[j] < -cut; });
-        }
-    } else {
-        // OpenMPManager.cpp:196-208
-        nu_p = nu_if;
-        const double rb = round((nu_if - cut - f0) / df);
-        const double re = round((nu_if + cut - f0) / df);
-        lo = clamp_index(rb > double(s) ? rb : double(s), s, e);
-        hi = clamp_index(re < double(e) ? re : double(e), s, e);
-    }
+    // step two reads the uploaded centre in the GPU convention
+    // (cross_kernal.cu:951), the nu = 0 guarded one in the CPU convention
+    const double nu_p = CONV == kConvGpu ? nu : nu_if;
     const double md = (nu_p - f0) / df;
     const double m = rint(md);
     const double nu_df = nu_p / df;  // q = 1 / (g df) = nu_df * dpw
     const bool far_m = !(fabs(m) < 16000000.0);
-    const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(i);
+    if (live) a.mi[i] = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
+
+    // device_compute_cross_section_voigt_stepone, cross_kernal.cu:775-779
+    // (GPU); OpenMPManager.cpp:196-200 (CPU)
+    auto class_values = [&](const CondDev& Cd, double& S, double& pw, double& g) {
+        S = Cd.cmcoef * aif * gns * kISQRTPI * exp(-Cd.beta * ei) * (1.0 - exp(-Cd.beta * nu_if)) /
+            (nu_if * nu_if * Cd.partition);
+        if (CONV == kConvGpu && gns == -1) S = aif;
+        pw = pow(Cd.tratio, nex);
+        g = 1.0 / (nu_p * Cd.dpw);  // gammaG, cross_kernal.cu:958
+    };
+    const int ncache = a.nclass <= kMaxClassCache ? a.nclass : 0;
+    double* cS = cls;
+    double* cP = cls + ncache * 256;
+    double* cG = cls + 2 * ncache * 256;
     if (live) {
-        if (cg == 0) a.mi[i] = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
-        LineShX ls;
-        ls.m = float(far_m ? 0.0 : m);
-        ls.dfn = float(df / nu_p);
-        ls.rn = float(((nu_p - f0) - m * df) / nu_p);
-        ls.whole = far_m ? 1 : 0;
-        ls.lo = lo;
-        ls.hi = hi;
-        ls.nu = nu_p;
-        reinterpret_cast<LineShX*>(a.lsh)[gi] = ls;
-        a.wlo[gi] = lo;
-        a.whi[gi] = hi;
+        for (int t = 0; t < ncache; ++t)
+            class_values(a.cond[a.class_rep[t]], cS[t * 256 + tid], cP[t * 256 + tid], cG[t * 256 + tid]);
     }
 
-    double S = 0.0, pw = 0.0, g = 0.0;
-    int prev_class = -1;
-    LineR1<C> lr;
-    LineIv<C> li;
-#pragma unroll
-    for (int k = 0; k < C; ++k) {
-        const int c = cg * C + k;
-        const CondDev& Cd = a.cond[c];
-        int kcl = 0, rch = 0;
+    double cut_prev = -1.0;
+    int lo = s, hi = s;
+    for (int cg = 0; cg < ngroups; ++cg) {
+        const double cut = a.cond[cg * C].cut;  // a group shares its cut
+        if (live && !(cut == cut_prev)) {
+            cut_prev = cut;
+            if (CONV == kConvGpu) {
+                // -cut <= nu - f <= cut (cross_kernal.cu:952-957)
+                lo = find_first(s, e, ceil((nu - cut - f0) / df), [&](int j) { return !(nu - F[j] > cut); });
+                hi = find_first(s, e, ceil((nu + cut - f0) / df), [&](int j) { return nu - F[j] < -cut; });
+            } else {
+                // OpenMPManager.cpp:196-208
+                const double rb = round((nu_if - cut - f0) / df);
+                const double re = round((nu_if + cut - f0) / df);
+                lo = clamp_index(rb > double(s) ? rb : double(s), s, e);
+                hi = clamp_index(re < double(e) ? re : double(e), s, e);
+            }
+        }
+        const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(live ? i : 0);
+        LineR1<C>& lr = reinterpret_cast<LineR1<C>*>(a.rec)[gi];
+        LineIv<C>& li = reinterpret_cast<LineIv<C>*>(a.liv)[gi];
         if (live) {
-            if (a.tclass[c] != prev_class) {
-                prev_class = a.tclass[c];
-                // device_compute_cross_section_voigt_stepone, cross_kernal.cu:775-779
-                // (GPU); OpenMPManager.cpp:196-200 (CPU)
-                S = Cd.cmcoef * aif * gns * kISQRTPI * exp(-Cd.beta * ei) *
-                    (1.0 - exp(-Cd.beta * nu_if)) / (nu_if * nu_if * Cd.partition);
-                if (CONV == kConvGpu && gns == -1) S = aif;
-                pw = pow(Cd.tratio, nex);
-                g = 1.0 / (nu_p * Cd.dpw);  // gammaG, cross_kernal.cu:958
+            LineShX ls;
+            ls.m = float(far_m ? 0.0 : m);
+            ls.dfn = float(df / nu_p);
+            ls.rn = float(((nu_p - f0) - m * df) / nu_p);
+            ls.whole = far_m ? 1 : 0;
+            ls.lo = lo;
+            ls.hi = hi;
+            ls.nu = nu_p;
+            reinterpret_cast<LineShX*>(a.lsh)[gi] = ls;
+            a.wlo[gi] = lo;
+            a.whi[gi] = hi;
+            if constexpr (C == 2) lr.pad[0] = lr.pad[1] = 0.0f;
+        }
+#pragma unroll 1
+        for (int k = 0; k < C; ++k) {
+            const int c = cg * C + k;
+            const CondDev& Cd = a.cond[c];
+            int kcl = 0, rch = 0;
+            if (live) {
+                double S, pw, g;
+                if (ncache) {
+                    const int t = a.tclass[c];
+                    S = cS[t * 256 + tid];
+                    pw = cP[t * 256 + tid];
+                    g = cG[t * 256 + tid];
+                } else {
+                    class_values(Cd, S, pw, g);
+                }
+                const double gl = gam * Cd.gamma_scale * pw;
+                const double y = gl * g;
+                const double pref = (CONV == kConvCpu && S == 0.0) ? 0.0 : S * g;
+                const double y2 = y * y;
+                const double Pc = pref * kW4C * y;
+                const double xw = (cut_prev + double(a.mixed_tile_span + 4) * df) * g;
+                const bool whole = far_m || !(xw < kWholeXMax);
+                CoreIv iv;
+                const double q = nu_df * Cd.dpw;
+                region_interval_q(nu_p, g, y, 15.0, lo, hi, f0, df, md, q, iv.lo15, iv.hi15);
+                region_interval_q(nu_p, g, y, 5.5, lo, hi, f0, df, md, q, iv.lo55, iv.hi55);
+                if (iv.lo15 <= iv.hi15) {
+                    const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
+                    rch = w < 3.0e7 ? int(w) : 30000000;
+                    if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
+                }
+                kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
+                const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
+                a.civ[ci] = iv;
+                a.cyp[ci] = make_float2(float(y), float(pref));
+                lr.Cy[k] = float(y2 - 0.5);
+                lr.D2[k] = float(2.0 * y2);
+                lr.Pc[k] = float(Pc);
+                li.lo[k] = iv.lo15;
+                li.hi[k] = iv.hi15;
             }
-            const double gl = gam * Cd.gamma_scale * pw;
-            const double y = gl * g;
-            const double pref = (CONV == kConvCpu && S == 0.0) ? 0.0 : S * g;
-            const double y2 = y * y;
-            const double Pc = pref * kW4C * y;
-            const double xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
-            const bool whole = far_m || !(xw < kWholeXMax);
-            CoreIv iv;
-            const double q = nu_df * Cd.dpw;
-            region_interval_q(nu_p, g, y, 15.0, lo, hi, f0, df, md, q, iv.lo15, iv.hi15);
-            region_interval_q(nu_p, g, y, 5.5, lo, hi, f0, df, md, q, iv.lo55, iv.hi55);
-            if (iv.lo15 <= iv.hi15) {
-                const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
-                rch = w < 3.0e7 ? int(w) : 30000000;
-                if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
+            kcl = __reduce_max_sync(0xffffffffu, kcl);
+            rch = __reduce_max_sync(0xffffffffu, rch);
+            if (lane == 0) {
+                smax[0][c][warp] = kcl;
+                smax[1][c][warp] = rch;
             }
-            kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
-            const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
-            a.civ[ci] = iv;
-            a.cyp[ci] = make_float2(float(y), float(pref));
-            lr.Cy[k] = float(y2 - 0.5);
-            lr.D2[k] = float(2.0 * y2);
-            lr.Pc[k] = float(Pc);
-            li.lo[k] = iv.lo15;
-            li.hi[k] = iv.hi15;
         }
-        kcl = __reduce_max_sync(0xffffffffu, kcl);
-        rch = __reduce_max_sync(0xffffffffu, rch);
-        if (lane == 0) {
-            smax[0][k][warp] = kcl;
-            smax[1][k][warp] = rch;
-        }
-    }
-    if (live) {
-        // the line's records of the group, stored whole (16-byte stores)
-        if constexpr (C == 2) {
-            lr.pad[0] = lr.pad[1] = 0.0f;
-        }
-        float4* dst = reinterpret_cast<float4*>(reinterpret_cast<LineR1<C>*>(a.rec) + gi);
-        const float4* src = reinterpret_cast<const float4*>(&lr);
-#pragma unroll
-        for (int q = 0; q < int(sizeof(LineR1<C>) / 16); ++q) dst[q] = src[q];
-        int4* idst = reinterpret_cast<int4*>(reinterpret_cast<LineIv<C>*>(a.liv) + gi);
-        const int4* isrc = reinterpret_cast<const int4*>(&li);
-#pragma unroll
-        for (int q = 0; q < int(sizeof(LineIv<C>) / 16); ++q) idst[q] = isrc[q];
     }
     // block maxima of the core-candidate widths (kc) and of the core pass's
     // reach (kc + kMaxCond), one atomic each per block and condition
     __syncthreads();
-    if (threadIdx.x < 2 * C) {
-        const int which = threadIdx.x / C, k = threadIdx.x % C;
+    for (int idx = tid; idx < 2 * a.ncond; idx += 256) {
+        const int which = idx / a.ncond, c = idx - which * a.ncond;
         int mx = 0;
 #pragma unroll
-        for (int w = 0; w < 4; ++w) mx = smax[which][k][w] > mx ? smax[which][k][w] : mx;
-        if (mx > 0) atomicMax(a.kc + (which ? kMaxCond : 0) + cg * C + k, mx);
+        for (int w = 0; w < 8; ++w) mx = smax[which][c][w] > mx ? smax[which][c][w] : mx;
+        if (mx > 0) atomicMax(a.kc + (which ? kMaxCond : 0) + c, mx);
     }
 }
 
@@ -2261,27 +2267,22 @@ cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaS
     const dim3 grid(unsigned((a.L.n + 255) / 256), unsigned(a.ncond));
     if (kind == kVoigt && mixed && a.group > 0) {
         // (precomputed-intensity lists run one condition at a time)
-        if (a.L.s32 != nullptr) return cudaErrorInvalidValue;
-        // one thread per (line, group), group fastest
-        const long ngroups = a.ncond / a.group;
-        const long nblk = (a.L.n + 127) / 128 * ngroups;
-        if (a.ncond % a.group != 0 || nblk > long(INT_MAX)) return cudaErrorInvalidValue;
-        const unsigned gx = unsigned(nblk);
+        if (a.L.s32 != nullptr || a.ncond % a.group != 0) return cudaErrorInvalidValue;
+        const unsigned nblk = unsigned((a.L.n + 255) / 256);
+        const int ncache = a.nclass <= kMaxClassCache ? a.nclass : 0;
+        const size_t smem = sizeof(double) * 3 * size_t(ncache) * 256;
+        auto go = [&](auto kernel) {
+            if (smem > 48 * 1024 &&
+                cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+                return cudaGetLastError();
+            kernel<<<nblk, 256, smem, stream>>>(a);
+            return cudaGetLastError();
+        };
         switch (a.group) {
-            case 2:
-                if (conv == kConvGpu) k_prep_group_x<kConvGpu, 2><<<gx, 128, 0, stream>>>(a);
-                else k_prep_group_x<kConvCpu, 2><<<gx, 128, 0, stream>>>(a);
-                break;
-            case 4:
-                if (conv == kConvGpu) k_prep_group_x<kConvGpu, 4><<<gx, 128, 0, stream>>>(a);
-                else k_prep_group_x<kConvCpu, 4><<<gx, 128, 0, stream>>>(a);
-                break;
-            case 8:
-                if (conv == kConvGpu) k_prep_group_x<kConvGpu, 8><<<gx, 128, 0, stream>>>(a);
-                else k_prep_group_x<kConvCpu, 8><<<gx, 128, 0, stream>>>(a);
-                break;
-            default:
-                return cudaErrorInvalidValue;
+            case 2: return conv == kConvGpu ? go(k_prep_lines_x<kConvGpu, 2>) : go(k_prep_lines_x<kConvCpu, 2>);
+            case 4: return conv == kConvGpu ? go(k_prep_lines_x<kConvGpu, 4>) : go(k_prep_lines_x<kConvCpu, 4>);
+            case 8: return conv == kConvGpu ? go(k_prep_lines_x<kConvGpu, 8>) : go(k_prep_lines_x<kConvCpu, 8>);
+            default: return cudaErrorInvalidValue;
         }
     } else if (kind == kVoigt) {
         if (conv == kConvGpu) {
