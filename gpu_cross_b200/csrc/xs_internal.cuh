@@ -110,11 +110,15 @@ struct __align__(16) LineShX {
     float m;      // nearest grid index (exact below 2^24)
     float dfn;    // df / nu
     float rn;     // (nu - f0 - m df) / nu
-    int whole;    // 1: X from nu in FP64 and every pair of the line tested
+    int flags;    // kLineWhole: X from nu in FP64 and every pair of the line
+                  // tested; kLineWide: region-I products need the scaled
+                  // shared reciprocal
     int lo, hi;   // window [lo, hi) of grid indices
     double nu;    // centre (whole lines)
 };
 static_assert(sizeof(LineShX) == 32, "LineShX layout");
+constexpr int kLineWhole = 1;
+constexpr int kLineWide = 2;
 // Region-I constants of a line for the C conditions of its group, each
 // array in condition order: conditions 2k and 2k+1 are one packed FP32x2
 // operand, conditions 4k..4k+3 one 16-byte load.  This is all step two

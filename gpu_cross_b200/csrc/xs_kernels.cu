@@ -40,6 +40,12 @@ constexpr double kWholeXMax = 1.0e8;
 // tau dA dB in [1.2e-22, 7.9e33] and its reciprocal in [1.3e-34, 8e21]: all
 // normal FP32 numbers.
 constexpr float kPairTau = 7.88860905221011805e-31f;
+// Lines whose x^2 + y^2 stays below kPairUMax over their tiles for every
+// condition of the group ("narrow" lines, the usual case) share reciprocals
+// without the scaling: their region-I denominators d = u^2 + 2 y^2 lie in
+// [1.2e4, 6.3e18], so dA dB lies in [1.5e8, 4e37] and its reciprocal is a
+// normal FP32 number.  Other lines are marked kLineWide.
+constexpr double kPairUMax = 2.5e9;
 
 
 // ---------------------------------------------------------------------------
@@ -527,19 +533,11 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
         LineR1<C>& lr = reinterpret_cast<LineR1<C>*>(a.rec)[gi];
         LineIv<C>& li = reinterpret_cast<LineIv<C>*>(a.liv)[gi];
         if (live) {
-            LineShX ls;
-            ls.m = float(far_m ? 0.0 : m);
-            ls.dfn = float(df / nu_p);
-            ls.rn = float(((nu_p - f0) - m * df) / nu_p);
-            ls.whole = far_m ? 1 : 0;
-            ls.lo = lo;
-            ls.hi = hi;
-            ls.nu = nu_p;
-            reinterpret_cast<LineShX*>(a.lsh)[gi] = ls;
             a.wlo[gi] = lo;
             a.whi[gi] = hi;
             if constexpr (C == 2) lr.pad[0] = lr.pad[1] = 0.0f;
         }
+        bool wide = false;
 #pragma unroll 1
         for (int k = 0; k < C; ++k) {
             const int c = cg * C + k;
@@ -562,6 +560,7 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                 const double Pc = pref * kW4C * y;
                 const double xw = (cut_prev + double(a.mixed_tile_span + 4) * df) * g;
                 const bool whole = far_m || !(xw < kWholeXMax);
+                wide = wide || !(xw * xw + y2 < kPairUMax);
                 CoreIv iv;
                 const double q = nu_df * Cd.dpw;
                 region_interval_q(nu_p, g, y, 15.0, lo, hi, f0, df, md, q, iv.lo15, iv.hi15);
@@ -587,6 +586,17 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                 smax[0][c][warp] = kcl;
                 smax[1][c][warp] = rch;
             }
+        }
+        if (live) {
+            LineShX ls;
+            ls.m = float(far_m ? 0.0 : m);
+            ls.dfn = float(df / nu_p);
+            ls.rn = float(((nu_p - f0) - m * df) / nu_p);
+            ls.flags = (far_m ? kLineWhole : 0) | (wide ? kLineWide : 0);
+            ls.lo = lo;
+            ls.hi = hi;
+            ls.nu = nu_p;
+            reinterpret_cast<LineShX*>(a.lsh)[gi] = ls;
         }
     }
     // block maxima of the core-candidate widths (kc) and of the core pass's
@@ -1586,14 +1596,13 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         const std::false_type plain;
         const std::true_type guarded;
         // Region I of two pairs of conditions (A, B) with one reciprocal per
-        // two line-evals: lane h of A and lane h of B share 1 / (tau dA dB),
-        // so 1/dA = (tau dB) / (tau dA dB) and 1/dB = (tau dA) / (tau dA dB)
-        // (kPairTau: every scaled value stays a normal FP32 number for the
-        // region-I pairs of lines that are not whole).  Pairs where `keep`
-        // is false add exactly zero.
-        // pA = 2q, pB = 2q + 1: conditions 4q..4q+3, one 16-byte load for
-        // each of Cy, D2 and Pc.
-        auto region1_ab = [&](float X2, const R1& r, int pA, int pB, bool keep) {
+        // two line-evals: lane h of A and lane h of B share 1 / (dA dB), so
+        // 1/dA = dB / (dA dB) and 1/dB = dA / (dA dB).  For narrow lines the
+        // product itself stays in range (kPairUMax); for wide ones both
+        // factors are scaled by kPairTau first, 1/dA = (tau dB) / (tau dA dB).
+        // pA = 2q, pB = 2q + 1: conditions 4q..4q+3, one 16-byte load for each
+        // of Cy, D2 and Pc.  Pairs where `keep` is false add exactly zero.
+        auto region1_ab = [&](auto narrow, float X2, const R1& r, int pA, int pB, bool keep) {
             const float4 cy = *reinterpret_cast<const float4*>(&r.Cy[2 * pA]);
             const float4 d2 = *reinterpret_cast<const float4*>(&r.D2[2 * pA]);
             const float4 pc = *reinterpret_cast<const float4*>(&r.Pc[2 * pA]);
@@ -1603,13 +1612,22 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             const float2 dB = __ffma2_rn(uB, uB, f2(d2.z, d2.w));
             const float2 nA = __ffma2_rn(uA, f2(pc.x, pc.y), f2(pc.x, pc.y));
             const float2 nB = __ffma2_rn(uB, f2(pc.z, pc.w), f2(pc.z, pc.w));
-            const float2 aA = __fmul2_rn(dA, f2s(kPairTau));
-            const float2 bB = __fmul2_rn(dB, f2s(kPairTau));
-            const float2 q = __fmul2_rn(aA, dB);
-            const float2 rq = keep ? f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)) : f2(0.0f, 0.0f);
-            acc[pA] = __ffma2_rn(nA, __fmul2_rn(bB, rq), acc[pA]);
-            acc[pB] = __ffma2_rn(nB, __fmul2_rn(aA, rq), acc[pB]);
+            if constexpr (decltype(narrow)::value) {
+                const float2 q = __fmul2_rn(dA, dB);
+                const float2 rq = keep ? f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)) : f2(0.0f, 0.0f);
+                acc[pA] = __ffma2_rn(nA, __fmul2_rn(dB, rq), acc[pA]);
+                acc[pB] = __ffma2_rn(nB, __fmul2_rn(dA, rq), acc[pB]);
+            } else {
+                const float2 aA = __fmul2_rn(dA, f2s(kPairTau));
+                const float2 bB = __fmul2_rn(dB, f2s(kPairTau));
+                const float2 q = __fmul2_rn(aA, dB);
+                const float2 rq = keep ? f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)) : f2(0.0f, 0.0f);
+                acc[pA] = __ffma2_rn(nA, __fmul2_rn(bB, rq), acc[pA]);
+                acc[pB] = __ffma2_rn(nB, __fmul2_rn(aA, rq), acc[pB]);
+            }
         };
+        const std::true_type narrow;
+        const std::false_type scaled;
 
         const int ngroups = split_groups(Lb - La, a.splits, split);
         auto gstart = [&](int gi) { return La + 32 * (split + gi * a.splits); };
@@ -1640,20 +1658,29 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             auto lo_of = [&](int v) { return (v < gb ? gb : (v > ge ? ge : v)) - gb; };
             const int a0 = lo_of(La), a1 = lo_of(fs), b1 = lo_of(E), c1 = lo_of(Fc), d1 = lo_of(fe),
                       e1 = lo_of(Lb);
+            // One line's region I at this lane's point, conditions in pairs
+            // of pairs (keep: the point takes the line).
+            auto line_region1 = [&](float X2, const R1& r, bool wide, bool keep) {
+                if constexpr (NP % 2 == 0) {
+                    if (!wide) {
+#pragma unroll
+                        for (int p = 0; p < NP; p += 2) region1_ab(narrow, X2, r, p, p + 1, keep);
+                    } else {
+#pragma unroll
+                        for (int p = 0; p < NP; p += 2) region1_ab(scaled, X2, r, p, p + 1, keep);
+                    }
+                } else {
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) region1(plain, X2, r, p, keep, keep);
+                }
+            };
             // Full lines away from every core: region I with no test.
             auto fast_run = [&](int x, int y) {
 #pragma unroll 2
                 for (int t = x; t < y; ++t) {
                     const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
                     const float X = fmaf(s.x - jf, s.y, s.z);
-                    const float X2 = X * X;
-                    if constexpr (NP % 2 == 0) {
-#pragma unroll
-                        for (int p = 0; p < NP; p += 2) region1_ab(X2, SR[t], p, p + 1, true);
-                    } else {
-#pragma unroll
-                        for (int p = 0; p < NP; ++p) region1(plain, X2, SR[t], p, true, true);
-                    }
+                    line_region1(X * X, SR[t], (__float_as_int(s.w) & kLineWide) != 0, true);
                 }
             };
             // Partial lines away from every core: the window as a lane mask.
@@ -1662,14 +1689,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
                     const bool in = jj >= SL[t].lo && jj < SL[t].hi && jj < t1;
                     const float X = fmaf(s.x - jf, s.y, s.z);
-                    const float X2 = X * X;
-                    if constexpr (NP % 2 == 0) {
-#pragma unroll
-                        for (int p = 0; p < NP; p += 2) region1_ab(X2, SR[t], p, p + 1, in);
-                    } else {
-#pragma unroll
-                        for (int p = 0; p < NP; ++p) region1(plain, X2, SR[t], p, in, in);
-                    }
+                    line_region1(X * X, SR[t], (__float_as_int(s.w) & kLineWide) != 0, in);
                 }
             };
             // Core candidates: region I outside each condition's interval.
@@ -1680,7 +1700,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
                     // whole lines: X from the FP64 centre (rare; the grid
                     // value is read here rather than held for every line)
-                    const float X = s.whole ? float((s.nu - a.G.freq[jj < t1 ? jj : tl]) / s.nu)
+                    const float X = (s.flags & kLineWhole) ? float((s.nu - a.G.freq[jj < t1 ? jj : tl]) / s.nu)
                                             : fmaf(s.m - jf, s.dfn, s.rn);
                     const float X2 = X * X;
                     const float aX = fabsf(X);
@@ -1801,7 +1821,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
                 const LineShX s = lsh[i];
                 const float2 yp = cyp[i];
                 for (int j = jlo; j <= jhi; ++j) {
-                    const float X = s.whole ? float((s.nu - a.freq[j]) / s.nu) : fmaf(s.m - float(j), s.dfn, s.rn);
+                    const float X = (s.flags & kLineWhole) ? float((s.nu - a.freq[j]) / s.nu)
+                                                           : fmaf(s.m - float(j), s.dfn, s.rn);
                     const float ax = fabsf(X) * k, y = yp.x;
                     float w;
                     if (j >= iv.lo55 && j <= iv.hi55)

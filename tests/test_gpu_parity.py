@@ -93,6 +93,28 @@ def test_line_splits_multi_condition(engine, cuda):
         assert_mixed_parity(five[k], f64[k])
 
 
+@pytest.mark.parametrize("C", [4, 8])
+def test_multi_condition_mixed_wide_and_narrow_lines(engine, cuda, C):
+    """Lines at 10-60 cm-1 have Doppler widths of a few 1e-5 cm-1, so the
+    25 cm-1 cut reaches x ~ 1e6: their shared region-I reciprocals need the
+    scaled products ("wide" lines); lines at 2000 cm-1 take the unscaled ones.
+    Mixed against FP64 for both in one call."""
+    low = synth.random_lines(1500, 10.0, 60.0, 2500.0, 1e-6, 1e2, seed=54, pressure_atm=1.0)
+    high = synth.random_lines(1500, 2000.0, 2050.0, 2500.0, 1e-6, 1e2, seed=55, pressure_atm=1.0)
+    lines = synth.LineList(*(np.concatenate([getattr(low, f), getattr(high, f)])
+                             for f in ("nu", "energies", "aif", "gns", "gamma", "n")))
+    grid = synth.Grid(0.0, 2100.0, 210000)
+    base = dict(mean_mass=17.03, pressure=1.0, ref_temp=296.0)
+    conds = [dict(base, temperature=t, partition=synth.partition_poly(t), gamma_scale=p, cut=25.0)
+             for t in (300.0, 2100.0) for p in (1e-3, 0.1, 1.0, 10.0)][:C]
+    fr = grid.freq()
+    f64 = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds)
+    mix = run_engine(engine, capi.VOIGT, lines, fr, base, grid.dfreq, cuda, conds=conds, C=C,
+                     precision=capi.MIXED)
+    for k in range(len(conds)):
+        assert_mixed_parity(mix[k], f64[k])
+
+
 @pytest.mark.parametrize("C", [2, 4, 8])
 def test_multi_condition_mixed_cpu_convention(engine, cuda, C):
     """Mixed multi-condition tiles in the CPU convention (sqrt(ln 2) Doppler
