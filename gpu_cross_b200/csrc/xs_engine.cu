@@ -641,7 +641,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.liv = reinterpret_cast<int*>(base + plan.off_liv);
 
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, ev_flags);
-        err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(2 * kMaxCond), st);
+        err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(kKcWords), st);
         if (err != cudaSuccess) return cuda_fail(err, "core-width reset");
         err = launch_prep(kind, opt->convention, mixed, pa, st);
         if (err != cudaSuccess) return cuda_fail(err, "step one launch");

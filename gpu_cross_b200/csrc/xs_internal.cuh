@@ -41,6 +41,10 @@ constexpr unsigned kErrGrid = 2u;
 constexpr unsigned kErrReach = 4u;
 
 constexpr int kMaxCond = 64;  // conditions per launch (the sweep uses 40)
+// Per-condition words step one reduces into (cleared before it runs): the
+// widest core-candidate band, the core pass's reach, and (single-condition
+// mixed layout) whether any line needs the scaled shared reciprocal.
+constexpr int kKcWords = 3 * kMaxCond;
 constexpr int kMaxSplits = 64;                      // line splits per tile
 constexpr size_t kMaxPartBytes = size_t(64) << 20;  // automatic splits' part buffer
 

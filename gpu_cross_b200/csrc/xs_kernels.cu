@@ -190,7 +190,10 @@ __device__ __forceinline__ void region_interval_q(double nu, double g, double y,
 // The mixed-precision multi-condition layout has its own step one
 // (k_prep_group_x); the FP64 one is written here.
 template <int KIND, int CONV, bool MIXED>
-__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* reach = nullptr) {
+// `wide` (mixed Voigt, single-condition layout): 1 when the line's region-I
+// products need the scaled shared reciprocal (kPairUMax).
+__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* reach = nullptr,
+                                         int* wide = nullptr) {
     const CondDev& C = a.cond[c];
     const double* F = a.G.freq;
     const double f0 = F[0];
@@ -287,8 +290,9 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
         // FP32 offsets need |m| < 2^24 and x below ~1e8 over the window;
         // otherwise every pair of the line takes the per-pair path.
         bool whole = false;
+        double xw = 0.0;
         if (MIXED) {
-            const double xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
+            xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
             whole = !(fabs(m) < 16000000.0) || !(xw < kWholeXMax);
         }
         if (whole) {
@@ -362,6 +366,7 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
                 if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
             }
             if (reach) *reach = rch;
+            if (wide) *wide = (!whole && !(xw * xw + y2 < kPairUMax)) ? 1 : 0;
             kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
             rr.clo = float(j15);
             rr.chi = float(k15);
@@ -424,23 +429,26 @@ template <int KIND, int CONV, bool MIXED>
 __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
-    int kcl = 0, rch = 0;
-    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, &rch);
+    int kcl = 0, rch = 0, wd = 0;
+    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, &rch, &wd);
     if (KIND == kVoigt) {
-        // Block maxima of the core widths (kc) and, mixed, of the core pass's
-        // reach (kc + kMaxCond), one atomic each per block.
-        __shared__ int smax[2][8];
+        // Block maxima of the core widths (kc), and, mixed, of the core
+        // pass's reach (kc + kMaxCond) and of the wide-line flag
+        // (kc + 2 kMaxCond), one atomic each per block.
+        __shared__ int smax[3][8];
         kcl = __reduce_max_sync(0xffffffffu, kcl);
         rch = __reduce_max_sync(0xffffffffu, rch);
+        wd = __reduce_max_sync(0xffffffffu, wd);
         if ((threadIdx.x & 31) == 0) {
             smax[0][threadIdx.x >> 5] = kcl;
             smax[1][threadIdx.x >> 5] = rch;
+            smax[2][threadIdx.x >> 5] = wd;
         }
         __syncthreads();
-        if (threadIdx.x < 2) {
+        if (threadIdx.x < 3) {
             int m = 0;
             for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[threadIdx.x][w] > m ? smax[threadIdx.x][w] : m;
-            if (m > 0) atomicMax(a.kc + (threadIdx.x ? kMaxCond : 0) + c, m);
+            if (m > 0) atomicMax(a.kc + threadIdx.x * kMaxCond + c, m);
         }
     }
 }
@@ -920,6 +928,9 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
         const int* wlo = a.wlo + cbase;
         const int* mi = a.mi;
         const int kc = a.kc[w.c];
+        // (mixed) no line of this condition needs the scaled shared
+        // reciprocal: region-I products are formed unscaled (kPairUMax)
+        const bool narrow_call = MIXED && a.kc[2 * kMaxCond + w.c] == 0;
         const int t0 = w.t0, t1 = w.t1, tl = t1 - 1;
         const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
         const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
@@ -967,12 +978,22 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
                         const float2 denB = __ffma2_rn(uB, uB, f2s(v1.x));
                         const float2 numA = __ffma2_rn(uA, f2s(v1.y), f2s(v1.y));
                         const float2 numB = __ffma2_rn(uB, f2s(v1.y), f2s(v1.y));
-                        const float2 aA = __fmul2_rn(denA, f2s(kPairTau));
-                        const float2 bB = __fmul2_rn(denB, f2s(kPairTau));
-                        const float2 q = __fmul2_rn(aA, denB);
-                        const float2 r = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
-                        const float2 accA = __ffma2_rn(numA, __fmul2_rn(bB, r), f2(accf[p], accf[p + 1]));
-                        const float2 accB = __ffma2_rn(numB, __fmul2_rn(aA, r), f2(accf[p + 2], accf[p + 3]));
+                        float2 iA, iB;  // 1 / denA, 1 / denB
+                        if (narrow_call) {
+                            const float2 q = __fmul2_rn(denA, denB);
+                            const float2 r = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
+                            iA = __fmul2_rn(denB, r);
+                            iB = __fmul2_rn(denA, r);
+                        } else {
+                            const float2 aA = __fmul2_rn(denA, f2s(kPairTau));
+                            const float2 bB = __fmul2_rn(denB, f2s(kPairTau));
+                            const float2 q = __fmul2_rn(aA, denB);
+                            const float2 r = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
+                            iA = __fmul2_rn(bB, r);
+                            iB = __fmul2_rn(aA, r);
+                        }
+                        const float2 accA = __ffma2_rn(numA, iA, f2(accf[p], accf[p + 1]));
+                        const float2 accB = __ffma2_rn(numB, iB, f2(accf[p + 2], accf[p + 3]));
                         accf[p] = accA.x;
                         accf[p + 1] = accA.y;
                         accf[p + 2] = accB.x;
@@ -1027,12 +1048,22 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             const float2 denB = __ffma2_rn(uB, uB, f2s(b1.x));
             const float2 numA = __ffma2_rn(uA, f2s(a1.y), f2s(a1.y));
             const float2 numB = __ffma2_rn(uB, f2s(b1.y), f2s(b1.y));
-            const float2 aA = __fmul2_rn(denA, f2s(kPairTau));
-            const float2 bB = __fmul2_rn(denB, f2s(kPairTau));
-            const float2 q = __fmul2_rn(aA, denB);
-            const float2 rr = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
-            float2 acc = __ffma2_rn(numA, __fmul2_rn(bB, rr), f2(accf[0], accf[P > 1 ? 1 : 0]));
-            acc = __ffma2_rn(numB, __fmul2_rn(aA, rr), acc);
+            float2 iA, iB;  // 1 / denA, 1 / denB
+            if (narrow_call) {
+                const float2 q = __fmul2_rn(denA, denB);
+                const float2 rr = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
+                iA = __fmul2_rn(denB, rr);
+                iB = __fmul2_rn(denA, rr);
+            } else {
+                const float2 aA = __fmul2_rn(denA, f2s(kPairTau));
+                const float2 bB = __fmul2_rn(denB, f2s(kPairTau));
+                const float2 q = __fmul2_rn(aA, denB);
+                const float2 rr = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
+                iA = __fmul2_rn(bB, rr);
+                iB = __fmul2_rn(aA, rr);
+            }
+            float2 acc = __ffma2_rn(numA, iA, f2(accf[0], accf[P > 1 ? 1 : 0]));
+            acc = __ffma2_rn(numB, iB, acc);
             accf[0] = acc.x;
             accf[P > 1 ? 1 : 0] = acc.y;
         };
@@ -2388,7 +2419,7 @@ ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_
     p.off_whi = al(p.off_wlo + sizeof(int) * n * nwin);
     p.off_mi = al(p.off_whi + sizeof(int) * n * nwin);
     p.off_kc = al(p.off_mi + sizeof(int) * n);
-    p.off_lsh = al(p.off_kc + sizeof(int) * size_t(2 * kMaxCond));
+    p.off_lsh = al(p.off_kc + sizeof(int) * size_t(kKcWords));
     const size_t lsh = mixed ? sizeof(LineShX) : sizeof(LineSh64);
     p.off_civ = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
     const bool core = mixed && group > 0;

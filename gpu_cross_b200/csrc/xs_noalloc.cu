@@ -190,7 +190,7 @@ extern "C" int xs_execute_noalloc(const xs_options* opt, const xs_condition* con
     // work counter and the core widths must start at zero; records, windows
     // and grid indices are rewritten.
     cudaError_t e = cudaMemsetAsync(words, 0, 2 * sizeof(unsigned), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(2 * xs::kMaxCond), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(xs::kKcWords), st);
     if (e == cudaSuccess) e = xs::launch_grid_check(G, words, st);
     if (e == cudaSuccess) e = xs::launch_prep(kind, opt->convention, mixed, pa, st);
     if (e == cudaSuccess) e = xs::launch_steptwo(kind, opt->convention, mixed, P, W, blocks, sa, st);

@@ -93,7 +93,7 @@ def test_line_splits_multi_condition(engine, cuda):
         assert_mixed_parity(five[k], f64[k])
 
 
-@pytest.mark.parametrize("C", [4, 8])
+@pytest.mark.parametrize("C", [1, 4, 8])
 def test_multi_condition_mixed_wide_and_narrow_lines(engine, cuda, C):
     """Lines at 10-60 cm-1 have Doppler widths of a few 1e-5 cm-1, so the
     25 cm-1 cut reaches x ~ 1e6: their shared region-I reciprocals need the
