@@ -638,7 +638,10 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.lsh = base + plan.off_lsh;
         pa.civ = reinterpret_cast<CoreIv*>(base + plan.off_civ);
         pa.cyp = reinterpret_cast<float2*>(base + plan.off_cyp);
-        pa.liv = reinterpret_cast<int*>(base + plan.off_liv);
+        // window slots: groups with the same cut (consecutive) share the
+        // first one's window data
+        for (int g = 0; CG && g < nc / CG; ++g)
+            pa.wslot[g] = (g > 0 && pa.cond[g * CG].cut == pa.cond[(g - 1) * CG].cut) ? pa.wslot[g - 1] : g;
 
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, ev_flags);
         err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(kKcWords), st);
@@ -678,7 +681,8 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
         if (CG) {
             sa.lsh = pa.lsh;
-            sa.liv = pa.liv;
+            sa.civ = pa.civ;
+            for (int g = 0; g < nc / CG; ++g) sa.wslot[g] = pa.wslot[g];
             sa.group = CG;
             sa.tiles_per_cond = (grid->points + 31) / 32;
             sa.n_items = sa.tiles_per_cond * (nc / CG) * S;
@@ -741,6 +745,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
                 ca.kx[c] = sa.kx[c];
                 ca.row[c] = sa.row[c];
             }
+            for (int g = 0; g < nc / CG; ++g) ca.wslot[g] = pa.wslot[g];
             err = launch_core_mcx(ca, nc, st);
             if (err != cudaSuccess) return cuda_fail(err, "core pass launch");
             ++launched;

@@ -138,14 +138,6 @@ struct __align__(16) LineR1<2> {
 };
 static_assert(sizeof(LineR1<8>) == 96 && sizeof(LineR1<4>) == 48 && sizeof(LineR1<2>) == 32,
               "LineR1 layout");
-// The grid indices [lo, hi] of the chunk where the line's |x| + y < 15 (W4
-// regions II-IV; empty: lo > hi), per condition of the group: step two
-// leaves those pairs to the core pass.  Read from memory (not staged) by the
-// core-candidate lines only.
-template <int C>
-struct __align__(16) LineIv {
-    int lo[C], hi[C];
-};
 // Bytes per (line, group) of the mixed multi-condition region-I records.
 constexpr size_t line_r1_bytes(int C) { return C == 8 ? 96 : (C == 4 ? 48 : 32); }
 // Per (line, condition) of the mixed multi-condition layout, for the core
@@ -220,7 +212,11 @@ struct PrepArgs {
                         // (LineShX mixed, LineSh64 FP64)
     CoreIv* civ;        // mixed multi-condition: region intervals and
     float2* cyp;        //   (y, pref) per (condition, line), condition-major
-    int* liv;           // mixed multi-condition: LineIv<group> per (line, group)
+    // Multi-condition layouts: the window slot of each group -- groups with
+    // the same cut (consecutive, conditions being ordered by cut) share one
+    // copy of the per-line window data (LineShX / LineSh64, lo, hi), that of
+    // the first group of their run.
+    int wslot[kMaxCond];
     // Temperature classes: conditions of one class have the same cmcoef,
     // beta, Q, T_ref/T and Doppler width, so their intensity, Lorentz
     // temperature power and 1/Doppler width are the same numbers.  tclass[c]
@@ -244,7 +240,9 @@ struct StepArgs {
     size_t out_stride;  // elements between conditions
     GridDev G;
     const void* lsh;    // multi-condition layout (LineShX mixed, LineSh64 FP64)
-    const int* liv;     // mixed multi-condition: LineIv<group> per (line, group)
+    const CoreIv* civ;  // mixed multi-condition: the core-candidate lines'
+                        // region intervals, per (condition, line)
+    int wslot[kMaxCond];  // window slot of each group (PrepArgs::wslot)
     int group;          // conditions per group (multi-condition kernel)
     int tiles_per_cond;
     int n_items;
@@ -281,7 +279,7 @@ size_t record_bytes(int kind, bool mixed);
 // `ncond` conditions of `n` lines, the per-line grid index and the
 // per-condition core widths; sections 256-byte aligned from `base_off`.
 struct ScratchPlan {
-    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, off_liv, need;
+    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, need;
 };
 ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off,
                          int group = 0);
@@ -310,6 +308,7 @@ struct CoreArgs {
     size_t part_stride;
     float kx[kMaxCond];  // 1 / dpw
     int row[kMaxCond];
+    int wslot[kMaxCond];  // window slot of each group (PrepArgs::wslot)
 };
 cudaError_t launch_core_mcx(const CoreArgs& a, int ncond, cudaStream_t stream);
 // The same for the single-condition mixed layout (RecV32 records; a.kx set;

@@ -459,13 +459,13 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
 // temperature class (conditions with the same beta, Q, T_ref/T and Doppler
 // width; the 40-condition sweep has 10) are computed once per line and kept
 // in shared memory (up to kMaxClassCache classes; beyond, each condition
-// computes its own); what a group's conditions share -- the window, the
-// condition-free offsets (LineShX) -- is written per group; the conditions
-// follow in order, their loop not unrolled, which keeps the code small.
-// Each value takes the FP64 path's operations in the same order (the W4
-// region intervals are the FP64 region choice).  A line's records of a
-// group (LineR1, LineIv) are contiguous and written by one thread within a
-// short time, so whole sectors reach memory.
+// computes its own); what groups with the same cut share -- the window, the
+// condition-free offsets (LineShX) -- is written once per run of such
+// groups; the conditions follow in order, their loop not unrolled, which
+// keeps the code small.  Each value takes the FP64 path's operations in the
+// same order (the W4 region intervals are the FP64 region choice).  A
+// line's LineR1 of a group is written by one thread within a short time, so
+// whole sectors reach memory.
 template <int CONV, int C>
 __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
     static_assert(C % 2 == 0, "conditions come in pairs");
@@ -519,33 +519,54 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
             class_values(a.cond[a.class_rep[t]], cS[t * 256 + tid], cP[t * 256 + tid], cG[t * 256 + tid]);
     }
 
+    // Window data (LineShX, lo, hi) once per run of groups with the same cut
+    // (a.wslot), written when the run ends: its wide flag covers every
+    // condition of the run.
     double cut_prev = -1.0;
     int lo = s, hi = s;
+    int slot = -1;
+    bool wide = false;
+    auto flush_window = [&]() {
+        if (!live || slot < 0) return;
+        const size_t wi = size_t(slot) * size_t(a.L.n) + size_t(i);
+        LineShX ls;
+        ls.m = float(far_m ? 0.0 : m);
+        ls.dfn = float(df / nu_p);
+        ls.rn = float(((nu_p - f0) - m * df) / nu_p);
+        ls.flags = (far_m ? kLineWhole : 0) | (wide ? kLineWide : 0);
+        ls.lo = lo;
+        ls.hi = hi;
+        ls.nu = nu_p;
+        reinterpret_cast<LineShX*>(a.lsh)[wi] = ls;
+        a.wlo[wi] = lo;
+        a.whi[wi] = hi;
+    };
     for (int cg = 0; cg < ngroups; ++cg) {
-        const double cut = a.cond[cg * C].cut;  // a group shares its cut
-        if (live && !(cut == cut_prev)) {
+        if (a.wslot[cg] != slot) {
+            flush_window();
+            slot = a.wslot[cg];
+            wide = false;
+            const double cut = a.cond[cg * C].cut;  // a run of groups shares its cut
             cut_prev = cut;
-            if (CONV == kConvGpu) {
-                // -cut <= nu - f <= cut (cross_kernal.cu:952-957)
-                lo = find_first(s, e, ceil((nu - cut - f0) / df), [&](int j) { return !(nu - F[j] > cut); });
-                hi = find_first(s, e, ceil((nu + cut - f0) / df), [&](int j) { return nu - F[j] < -cut; });
-            } else {
-                // OpenMPManager.cpp:196-208
-                const double rb = round((nu_if - cut - f0) / df);
-                const double re = round((nu_if + cut - f0) / df);
-                lo = clamp_index(rb > double(s) ? rb : double(s), s, e);
-                hi = clamp_index(re < double(e) ? re : double(e), s, e);
+            if (live) {
+                if (CONV == kConvGpu) {
+                    // -cut <= nu - f <= cut (cross_kernal.cu:952-957)
+                    lo = find_first(s, e, ceil((nu - cut - f0) / df), [&](int j) { return !(nu - F[j] > cut); });
+                    hi = find_first(s, e, ceil((nu + cut - f0) / df), [&](int j) { return nu - F[j] < -cut; });
+                } else {
+                    // OpenMPManager.cpp:196-208
+                    const double rb = round((nu_if - cut - f0) / df);
+                    const double re = round((nu_if + cut - f0) / df);
+                    lo = clamp_index(rb > double(s) ? rb : double(s), s, e);
+                    hi = clamp_index(re < double(e) ? re : double(e), s, e);
+                }
             }
         }
         const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(live ? i : 0);
         LineR1<C>& lr = reinterpret_cast<LineR1<C>*>(a.rec)[gi];
-        LineIv<C>& li = reinterpret_cast<LineIv<C>*>(a.liv)[gi];
-        if (live) {
-            a.wlo[gi] = lo;
-            a.whi[gi] = hi;
-            if constexpr (C == 2) lr.pad[0] = lr.pad[1] = 0.0f;
+        if constexpr (C == 2) {
+            if (live) lr.pad[0] = lr.pad[1] = 0.0f;
         }
-        bool wide = false;
 #pragma unroll 1
         for (int k = 0; k < C; ++k) {
             const int c = cg * C + k;
@@ -585,8 +606,6 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                 lr.Cy[k] = float(y2 - 0.5);
                 lr.D2[k] = float(2.0 * y2);
                 lr.Pc[k] = float(Pc);
-                li.lo[k] = iv.lo15;
-                li.hi[k] = iv.hi15;
             }
             kcl = __reduce_max_sync(0xffffffffu, kcl);
             rch = __reduce_max_sync(0xffffffffu, rch);
@@ -595,18 +614,8 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                 smax[1][c][warp] = rch;
             }
         }
-        if (live) {
-            LineShX ls;
-            ls.m = float(far_m ? 0.0 : m);
-            ls.dfn = float(df / nu_p);
-            ls.rn = float(((nu_p - f0) - m * df) / nu_p);
-            ls.flags = (far_m ? kLineWhole : 0) | (wide ? kLineWide : 0);
-            ls.lo = lo;
-            ls.hi = hi;
-            ls.nu = nu_p;
-            reinterpret_cast<LineShX*>(a.lsh)[gi] = ls;
-        }
     }
+    flush_window();
     // block maxima of the core-candidate widths (kc) and of the core pass's
     // reach (kc + kMaxCond), one atomic each per block and condition
     __syncthreads();
@@ -1575,8 +1584,9 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         const int t1 = t0 + 32 < end ? t0 + 32 : end;
         const int tl = t1 - 1;
         const size_t gbase = size_t(cg) * size_t(a.n);
-        const int* whi = a.whi + gbase;
-        const int* wlo = a.wlo + gbase;
+        const size_t wbase = size_t(a.wslot[cg]) * size_t(a.n);  // the group's window data
+        const int* whi = a.whi + wbase;
+        const int* wlo = a.wlo + wbase;
         const int* mi = a.mi;
         int kc = 0;
 #pragma unroll
@@ -1589,9 +1599,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         const int fe = Cb > fs ? Cb : fs;
         const int E = int(warp_lower_bound(La, Lb, lane, [&](long i) { return mi[i] >= t0 - kc; }));
         const int Fc = int(warp_lower_bound(E, Lb, lane, [&](long i) { return mi[i] > tl + kc; }));
-        const LineShX* lsh = reinterpret_cast<const LineShX*>(a.lsh) + gbase;
+        const LineShX* lsh = reinterpret_cast<const LineShX*>(a.lsh) + wbase;
         const R1* r1 = reinterpret_cast<const R1*>(a.rec) + gbase;
-        const LineIv<C>* ivl = reinterpret_cast<const LineIv<C>*>(a.liv) + gbase;
 
         const int jj = t0 + lane;
         const float jf = float(jj);
@@ -1735,17 +1744,20 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                                             : fmaf(s.m - jf, s.dfn, s.rn);
                     const float X2 = X * X;
                     const float aX = fabsf(X);
-                    const LineIv<C> iv = ivl[gb + t];  // the conditions' core intervals
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
                         bool keep[2];
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
-                            const int c = 2 * p + h;
+                            const int c = cg * C + 2 * p + h;
+                            // the condition's core interval [lo15, hi15] (the
+                            // core pass's pairs), read from memory: core
+                            // candidates are a small share of the lines
+                            const int2 iv = *reinterpret_cast<const int2*>(
+                                &a.civ[size_t(c) * size_t(a.n) + size_t(gb + t)]);
                             // beyond x ~ 1e9 (lines far off the FP32 offset
                             // range) region I is taken as 0
-                            keep[h] = in && !(jj >= iv.lo[c] && jj <= iv.hi[c]) &&
-                                      aX * a.kx[cg * C + c] < 1.0e9f;
+                            keep[h] = in && !(jj >= iv.x && jj <= iv.y) && aX * a.kx[c] < 1.0e9f;
                         }
                         region1(guarded, X2, SR[t], p, keep[0], keep[1]);
                     }
@@ -1837,7 +1849,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     const long F = warp_lower_bound(E, a.n, lane, [&](long i) { return a.mi[i] > tl + K; });
     const CoreIv* civ = a.civ + size_t(c) * size_t(a.n);
     const float2* cyp = a.cyp + size_t(c) * size_t(a.n);
-    const LineShX* lsh = a.lsh + size_t(c / a.group) * size_t(a.n);
+    const LineShX* lsh = a.lsh + size_t(a.wslot[c / a.group]) * size_t(a.n);
     const float k = a.kx[c];
     const int split = int(blockIdx.z), S = a.splits;
     double acc = 0.0;
@@ -2424,8 +2436,7 @@ ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_
     p.off_civ = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
     const bool core = mixed && group > 0;
     p.off_cyp = al(p.off_civ + (core ? sizeof(CoreIv) * n * size_t(ncond) : 0));
-    p.off_liv = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
-    p.need = al(p.off_liv + (core ? 2 * sizeof(int) * size_t(group) * n * nwin : 0));
+    p.need = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
     return p;
 }
 
