@@ -640,6 +640,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.cyp = reinterpret_cast<float2*>(base + plan.off_cyp);
         // window slots: groups with the same cut (consecutive) share the
         // first one's window data
+        pa.liv = reinterpret_cast<int*>(base + plan.off_liv);
         for (int g = 0; CG && g < nc / CG; ++g)
             pa.wslot[g] = (g > 0 && pa.cond[g * CG].cut == pa.cond[(g - 1) * CG].cut) ? pa.wslot[g - 1] : g;
 
@@ -681,7 +682,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
         if (CG) {
             sa.lsh = pa.lsh;
-            sa.civ = pa.civ;
+            sa.liv = pa.liv;
             for (int g = 0; g < nc / CG; ++g) sa.wslot[g] = pa.wslot[g];
             sa.group = CG;
             sa.tiles_per_cond = (grid->points + 31) / 32;

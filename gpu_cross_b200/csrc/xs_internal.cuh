@@ -42,9 +42,8 @@ constexpr unsigned kErrReach = 4u;
 
 constexpr int kMaxCond = 64;  // conditions per launch (the sweep uses 40)
 // Per-condition words step one reduces into (cleared before it runs): the
-// widest core-candidate band, the core pass's reach, and (single-condition
-// mixed layout) whether any line needs the scaled shared reciprocal.
-constexpr int kKcWords = 3 * kMaxCond;
+// widest core-candidate band and the core pass's reach.
+constexpr int kKcWords = 2 * kMaxCond;
 constexpr int kMaxSplits = 64;                      // line splits per tile
 constexpr size_t kMaxPartBytes = size_t(64) << 20;  // automatic splits' part buffer
 
@@ -138,6 +137,15 @@ struct __align__(16) LineR1<2> {
 };
 static_assert(sizeof(LineR1<8>) == 96 && sizeof(LineR1<4>) == 48 && sizeof(LineR1<2>) == 32,
               "LineR1 layout");
+// The grid indices [lo, hi] of the chunk where the line's |x| + y < 15 (W4
+// regions II-IV; empty: lo > hi), per condition of the group: step two
+// leaves those pairs to the core pass.  Read from memory (not staged) by the
+// core-candidate lines only; line-major, so that one line's intervals are
+// one contiguous read.
+template <int C>
+struct __align__(16) LineIv {
+    int lo[C], hi[C];
+};
 // Bytes per (line, group) of the mixed multi-condition region-I records.
 constexpr size_t line_r1_bytes(int C) { return C == 8 ? 96 : (C == 4 ? 48 : 32); }
 // Per (line, condition) of the mixed multi-condition layout, for the core
@@ -217,6 +225,7 @@ struct PrepArgs {
     // copy of the per-line window data (LineShX / LineSh64, lo, hi), that of
     // the first group of their run.
     int wslot[kMaxCond];
+    int* liv;           // mixed multi-condition: LineIv<group> per (line, group)
     // Temperature classes: conditions of one class have the same cmcoef,
     // beta, Q, T_ref/T and Doppler width, so their intensity, Lorentz
     // temperature power and 1/Doppler width are the same numbers.  tclass[c]
@@ -240,8 +249,7 @@ struct StepArgs {
     size_t out_stride;  // elements between conditions
     GridDev G;
     const void* lsh;    // multi-condition layout (LineShX mixed, LineSh64 FP64)
-    const CoreIv* civ;  // mixed multi-condition: the core-candidate lines'
-                        // region intervals, per (condition, line)
+    const int* liv;     // mixed multi-condition: LineIv<group> per (line, group)
     int wslot[kMaxCond];  // window slot of each group (PrepArgs::wslot)
     int group;          // conditions per group (multi-condition kernel)
     int tiles_per_cond;
@@ -279,7 +287,7 @@ size_t record_bytes(int kind, bool mixed);
 // `ncond` conditions of `n` lines, the per-line grid index and the
 // per-condition core widths; sections 256-byte aligned from `base_off`.
 struct ScratchPlan {
-    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, need;
+    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, off_liv, need;
 };
 ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off,
                          int group = 0);

@@ -190,10 +190,7 @@ __device__ __forceinline__ void region_interval_q(double nu, double g, double y,
 // The mixed-precision multi-condition layout has its own step one
 // (k_prep_group_x); the FP64 one is written here.
 template <int KIND, int CONV, bool MIXED>
-// `wide` (mixed Voigt, single-condition layout): 1 when the line's region-I
-// products need the scaled shared reciprocal (kPairUMax).
-__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* reach = nullptr,
-                                         int* wide = nullptr) {
+__device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* reach = nullptr) {
     const CondDev& C = a.cond[c];
     const double* F = a.G.freq;
     const double f0 = F[0];
@@ -290,9 +287,8 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
         // FP32 offsets need |m| < 2^24 and x below ~1e8 over the window;
         // otherwise every pair of the line takes the per-pair path.
         bool whole = false;
-        double xw = 0.0;
         if (MIXED) {
-            xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
+            const double xw = (cut + double(a.mixed_tile_span + 4) * df) * g;
             whole = !(fabs(m) < 16000000.0) || !(xw < kWholeXMax);
         }
         if (whole) {
@@ -366,7 +362,6 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
                 if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
             }
             if (reach) *reach = rch;
-            if (wide) *wide = (!whole && !(xw * xw + y2 < kPairUMax)) ? 1 : 0;
             kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
             rr.clo = float(j15);
             rr.chi = float(k15);
@@ -429,23 +424,20 @@ template <int KIND, int CONV, bool MIXED>
 __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
-    int kcl = 0, rch = 0, wd = 0;
-    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, &rch, &wd);
+    int kcl = 0, rch = 0;
+    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, &rch);
     if (KIND == kVoigt) {
-        // Block maxima of the core widths (kc), and, mixed, of the core
-        // pass's reach (kc + kMaxCond) and of the wide-line flag
-        // (kc + 2 kMaxCond), one atomic each per block.
-        __shared__ int smax[3][8];
+        // Block maxima of the core widths (kc) and, mixed, of the core pass's
+        // reach (kc + kMaxCond), one atomic each per block.
+        __shared__ int smax[2][8];
         kcl = __reduce_max_sync(0xffffffffu, kcl);
         rch = __reduce_max_sync(0xffffffffu, rch);
-        wd = __reduce_max_sync(0xffffffffu, wd);
         if ((threadIdx.x & 31) == 0) {
             smax[0][threadIdx.x >> 5] = kcl;
             smax[1][threadIdx.x >> 5] = rch;
-            smax[2][threadIdx.x >> 5] = wd;
         }
         __syncthreads();
-        if (threadIdx.x < 3) {
+        if (threadIdx.x < 2) {
             int m = 0;
             for (int w = 0; w < int(blockDim.x >> 5); ++w) m = smax[threadIdx.x][w] > m ? smax[threadIdx.x][w] : m;
             if (m > 0) atomicMax(a.kc + threadIdx.x * kMaxCond + c, m);
@@ -464,8 +456,8 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
 // groups; the conditions follow in order, their loop not unrolled, which
 // keeps the code small.  Each value takes the FP64 path's operations in the
 // same order (the W4 region intervals are the FP64 region choice).  A
-// line's LineR1 of a group is written by one thread within a short time, so
-// whole sectors reach memory.
+// line's records of a group (LineR1, LineIv) are written by one thread
+// within a short time, so whole sectors reach memory.
 template <int CONV, int C>
 __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
     static_assert(C % 2 == 0, "conditions come in pairs");
@@ -564,6 +556,7 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
         }
         const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(live ? i : 0);
         LineR1<C>& lr = reinterpret_cast<LineR1<C>*>(a.rec)[gi];
+        LineIv<C>& li = reinterpret_cast<LineIv<C>*>(a.liv)[gi];
         if constexpr (C == 2) {
             if (live) lr.pad[0] = lr.pad[1] = 0.0f;
         }
@@ -606,6 +599,8 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                 lr.Cy[k] = float(y2 - 0.5);
                 lr.D2[k] = float(2.0 * y2);
                 lr.Pc[k] = float(Pc);
+                li.lo[k] = iv.lo15;
+                li.hi[k] = iv.hi15;
             }
             kcl = __reduce_max_sync(0xffffffffu, kcl);
             rch = __reduce_max_sync(0xffffffffu, rch);
@@ -937,9 +932,6 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
         const int* wlo = a.wlo + cbase;
         const int* mi = a.mi;
         const int kc = a.kc[w.c];
-        // (mixed) no line of this condition needs the scaled shared
-        // reciprocal: region-I products are formed unscaled (kPairUMax)
-        const bool narrow_call = MIXED && a.kc[2 * kMaxCond + w.c] == 0;
         const int t0 = w.t0, t1 = w.t1, tl = t1 - 1;
         const long La = warp_lower_bound(0, a.n, lane, [&](long i) { return whi[i] > t0; });
         const long Lb = warp_lower_bound(La, a.n, lane, [&](long i) { return wlo[i] >= t1; });
@@ -970,45 +962,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             if (MIXED) {
                 const float4* q = reinterpret_cast<const float4*>(&r);
                 const float4 v0 = q[0], v1 = q[1];
-                if constexpr (P % 4 == 0) {
-                    // rows (p, p+1) and (p+2, p+3) share one reciprocal per
-                    // two line-evals, as region1_ab in k_steptwo_voigt_mcx
-                    // (region I of a line that is not whole: the scaled
-                    // products stay normal, see kPairTau)
-#pragma unroll
-                    for (int p = 0; p < P; p += 4) {
-                        const float2 dA = __fadd2_rn(f2s(v0.x), f2(-jf[p], -jf[p + 1]));
-                        const float2 dB = __fadd2_rn(f2s(v0.x), f2(-jf[p + 2], -jf[p + 3]));
-                        const float2 xA = __ffma2_rn(dA, f2s(v0.z), f2s(v0.y));
-                        const float2 xB = __ffma2_rn(dB, f2s(v0.z), f2s(v0.y));
-                        const float2 uA = __ffma2_rn(xA, xA, f2s(v0.w));
-                        const float2 uB = __ffma2_rn(xB, xB, f2s(v0.w));
-                        const float2 denA = __ffma2_rn(uA, uA, f2s(v1.x));
-                        const float2 denB = __ffma2_rn(uB, uB, f2s(v1.x));
-                        const float2 numA = __ffma2_rn(uA, f2s(v1.y), f2s(v1.y));
-                        const float2 numB = __ffma2_rn(uB, f2s(v1.y), f2s(v1.y));
-                        float2 iA, iB;  // 1 / denA, 1 / denB
-                        if (narrow_call) {
-                            const float2 q = __fmul2_rn(denA, denB);
-                            const float2 r = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
-                            iA = __fmul2_rn(denB, r);
-                            iB = __fmul2_rn(denA, r);
-                        } else {
-                            const float2 aA = __fmul2_rn(denA, f2s(kPairTau));
-                            const float2 bB = __fmul2_rn(denB, f2s(kPairTau));
-                            const float2 q = __fmul2_rn(aA, denB);
-                            const float2 r = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
-                            iA = __fmul2_rn(bB, r);
-                            iB = __fmul2_rn(aA, r);
-                        }
-                        const float2 accA = __ffma2_rn(numA, iA, f2(accf[p], accf[p + 1]));
-                        const float2 accB = __ffma2_rn(numB, iB, f2(accf[p + 2], accf[p + 3]));
-                        accf[p] = accA.x;
-                        accf[p + 1] = accA.y;
-                        accf[p + 2] = accB.x;
-                        accf[p + 3] = accB.y;
-                    }
-                } else if constexpr (P % 2 == 0) {
+                if constexpr (P % 2 == 0) {
 #pragma unroll
                     for (int p = 0; p < P; p += 2) {
                         const float2 d = __fadd2_rn(f2s(v0.x), f2(-jf[p], -jf[p + 1]));
@@ -1039,42 +993,6 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
                     accd[p] = fma(fma(u, v2.x, v2.x), rcp_refined_f64(fma(u, u, v1.y)), accd[p]);
                 }
             }
-        };
-        // Two full lines away from every core at two rows per thread
-        // (mixed, P == 2): row pair (0, 1) of line A and of line B share one
-        // reciprocal per two line-evals, as region1_ab in
-        // k_steptwo_voigt_mcx; A's terms are added before B's.
-        auto fast_line2 = [&](const REC& rA, const REC& rB) {
-            const float4* qa = reinterpret_cast<const float4*>(&rA);
-            const float4* qb = reinterpret_cast<const float4*>(&rB);
-            const float4 a0 = qa[0], a1 = qa[1], b0 = qb[0], b1 = qb[1];
-            const float2 nj = f2(-jf[0], -jf[1]);
-            const float2 xA = __ffma2_rn(__fadd2_rn(f2s(a0.x), nj), f2s(a0.z), f2s(a0.y));
-            const float2 xB = __ffma2_rn(__fadd2_rn(f2s(b0.x), nj), f2s(b0.z), f2s(b0.y));
-            const float2 uA = __ffma2_rn(xA, xA, f2s(a0.w));
-            const float2 uB = __ffma2_rn(xB, xB, f2s(b0.w));
-            const float2 denA = __ffma2_rn(uA, uA, f2s(a1.x));
-            const float2 denB = __ffma2_rn(uB, uB, f2s(b1.x));
-            const float2 numA = __ffma2_rn(uA, f2s(a1.y), f2s(a1.y));
-            const float2 numB = __ffma2_rn(uB, f2s(b1.y), f2s(b1.y));
-            float2 iA, iB;  // 1 / denA, 1 / denB
-            if (narrow_call) {
-                const float2 q = __fmul2_rn(denA, denB);
-                const float2 rr = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
-                iA = __fmul2_rn(denB, rr);
-                iB = __fmul2_rn(denA, rr);
-            } else {
-                const float2 aA = __fmul2_rn(denA, f2s(kPairTau));
-                const float2 bB = __fmul2_rn(denB, f2s(kPairTau));
-                const float2 q = __fmul2_rn(aA, denB);
-                const float2 rr = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
-                iA = __fmul2_rn(bB, rr);
-                iB = __fmul2_rn(aA, rr);
-            }
-            float2 acc = __ffma2_rn(numA, iA, f2(accf[0], accf[P > 1 ? 1 : 0]));
-            acc = __ffma2_rn(numB, iB, acc);
-            accf[0] = acc.x;
-            accf[P > 1 ? 1 : 0] = acc.y;
         };
         // `full`: the line's window covers the whole tile.
         auto slow_line = [&](const REC& r, bool full) {
@@ -1277,22 +1195,14 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_min_blocks<P, WARPS, MIXED>
             {
                 int t = a1;
                 for (; t + 1 < b1; t += 2) {
-                    if constexpr (MIXED && P == 2) {
-                        fast_line2(R[t], R[t + 1]);
-                    } else {
-                        fast_line(R[t]);
-                        fast_line(R[t + 1]);
-                    }
+                    fast_line(R[t]);
+                    fast_line(R[t + 1]);
                 }
                 if (t < b1) fast_line(R[t]);
                 t = c1;
                 for (; t + 1 < d1; t += 2) {
-                    if constexpr (MIXED && P == 2) {
-                        fast_line2(R[t], R[t + 1]);
-                    } else {
-                        fast_line(R[t]);
-                        fast_line(R[t + 1]);
-                    }
+                    fast_line(R[t]);
+                    fast_line(R[t + 1]);
                 }
                 if (t < d1) fast_line(R[t]);
             }
@@ -1601,6 +1511,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         const int Fc = int(warp_lower_bound(E, Lb, lane, [&](long i) { return mi[i] > tl + kc; }));
         const LineShX* lsh = reinterpret_cast<const LineShX*>(a.lsh) + wbase;
         const R1* r1 = reinterpret_cast<const R1*>(a.rec) + gbase;
+        const LineIv<C>* ivl = reinterpret_cast<const LineIv<C>*>(a.liv) + gbase;
 
         const int jj = t0 + lane;
         const float jf = float(jj);
@@ -1744,20 +1655,20 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                                             : fmaf(s.m - jf, s.dfn, s.rn);
                     const float X2 = X * X;
                     const float aX = fabsf(X);
+                    // the conditions' core intervals (the core pass's pairs),
+                    // read from memory: core candidates are a small share of
+                    // the lines
+                    const LineIv<C> iv = ivl[gb + t];
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
                         bool keep[2];
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
-                            const int c = cg * C + 2 * p + h;
-                            // the condition's core interval [lo15, hi15] (the
-                            // core pass's pairs), read from memory: core
-                            // candidates are a small share of the lines
-                            const int2 iv = *reinterpret_cast<const int2*>(
-                                &a.civ[size_t(c) * size_t(a.n) + size_t(gb + t)]);
+                            const int c = 2 * p + h;
                             // beyond x ~ 1e9 (lines far off the FP32 offset
                             // range) region I is taken as 0
-                            keep[h] = in && !(jj >= iv.x && jj <= iv.y) && aX * a.kx[c] < 1.0e9f;
+                            keep[h] = in && !(jj >= iv.lo[c] && jj <= iv.hi[c]) &&
+                                      aX * a.kx[cg * C + c] < 1.0e9f;
                         }
                         region1(guarded, X2, SR[t], p, keep[0], keep[1]);
                     }
@@ -2436,7 +2347,8 @@ ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_
     p.off_civ = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
     const bool core = mixed && group > 0;
     p.off_cyp = al(p.off_civ + (core ? sizeof(CoreIv) * n * size_t(ncond) : 0));
-    p.need = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
+    p.off_liv = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
+    p.need = al(p.off_liv + (core ? 2 * sizeof(int) * size_t(group) * n * nwin : 0));
     return p;
 }
 
