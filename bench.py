@@ -881,7 +881,7 @@ def run_serving(args, dev_index: int):
     trace = synth.serving_trace(rate=args.serve_rate, duration_s=args.serve_seconds)
     log(f"[serve] {len(mols)} molecules ({sum(len(l) for l, _ in mols):.3e} lines) and "
         f"{len(trace)} requests generated in {time.perf_counter() - t0:.1f} s")
-    srv = capi.Server(dev_index)
+    srv = capi.Server(dev_index, policy=args.serve_policy)
     try:
         mids = [srv.add_molecule(l, m) for l, m in mols]
         del mols
@@ -968,7 +968,8 @@ def run_serving(args, dev_index: int):
                      f"{args.serve_seconds:g} s (seed 1005); molecules "
                      f"{'/'.join(f'{n * args.serve_scale:.0e}' for n, _ in synth.SERVE_MOLECULES)} "
                      "lines (M 18.02/30.01/16.04), T U(200,3000) K, P logU(1e-5,100) bar, "
-                     "Doppler/Voigt 1:1, span U(100,5000) cm-1, df logU(0.01,1) cm-1, cut 25")
+                     "Doppler/Voigt 1:1, span U(100,5000) cm-1, df logU(0.01,1) cm-1, cut 25; "
+                     f"chunk order {'round robin' if args.serve_policy else 'least remaining work'}")
     res["line_evals"] = "window-overlap count (line, point) pairs inside +/-25 cm-1"
     return res
 
@@ -1101,6 +1102,8 @@ def main():
                     help="default run: leave out the single-point and Doppler configurations")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-policy", type=int, default=0,
+                    help="server chunk order: 0 least remaining work, 1 round robin")
     ap.add_argument("--serve-alone", type=int, default=40,
                     help="heaviest requests timed alone for the p99 lower bound")
     ap.add_argument("--serve-scale", type=float, default=1.0,

@@ -15,6 +15,7 @@ from . import build as _build
 XS_OK = 0
 XS_ERR_INVALID, XS_ERR_CUDA, XS_ERR_NOMEM, XS_ERR_UNSORTED, XS_ERR_GRID = 1, 2, 3, 4, 5
 XS_ERR_STATE, XS_ERR_NODEVICE, XS_ERR_TIMEOUT, XS_ERR_UNSUPPORTED = 6, 7, 8, 9
+POLICY_LEAST_WORK, POLICY_ROUND_ROBIN = 0, 1
 
 GAUSSIAN, DOPPLER, VOIGT, PSUEDO_VOIGT = 0, 1, 2, 3
 CONV_GPU, CONV_CPU = 0, 1
@@ -69,7 +70,7 @@ class GridC(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device_budget", ctypes.c_size_t), ("host_budget", ctypes.c_size_t),
                 ("lanes", ctypes.c_int), ("depth", ctypes.c_int), ("chunk_pairs", ctypes.c_double),
-                ("chunk_lines", ctypes.c_size_t)]
+                ("chunk_lines", ctypes.c_size_t), ("policy", ctypes.c_int)]
 
 
 class Request(ctypes.Structure):
@@ -455,8 +456,9 @@ class Server:
     """A request server (xs_server_*): resident molecules, submit/wait."""
 
     def __init__(self, device: int = 0, device_budget: int = 0, host_budget: int = 0,
-                 lanes: int = 0, depth: int = 0, chunk_pairs: float = 0.0, chunk_lines: int = 0):
-        cfg = ServerConfig(device_budget, host_budget, lanes, depth, chunk_pairs, chunk_lines)
+                 lanes: int = 0, depth: int = 0, chunk_pairs: float = 0.0, chunk_lines: int = 0,
+                 policy: int = 0):
+        cfg = ServerConfig(device_budget, host_budget, lanes, depth, chunk_pairs, chunk_lines, policy)
         h = ctypes.c_void_p()
         check(lib().xs_server_create(device, ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h

@@ -1579,6 +1579,30 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         };
         const std::true_type narrow;
         const std::false_type scaled;
+        // region1_ab for a narrow core-candidate line, each condition with its
+        // own keep: a condition's pair that is not kept (inside its core
+        // interval or outside the window) enters the shared product as 1 and
+        // adds exactly zero, so the kept ones keep their region-I ranges.
+        auto region1_ab_keep = [&](float X2, const R1& r, int pA, int pB, bool q0, bool q1, bool q2,
+                                   bool q3) {
+            const float4 cy = *reinterpret_cast<const float4*>(&r.Cy[2 * pA]);
+            const float4 d2 = *reinterpret_cast<const float4*>(&r.D2[2 * pA]);
+            const float4 pc = *reinterpret_cast<const float4*>(&r.Pc[2 * pA]);
+            const float2 uA = __ffma2_rn(f2(X2, X2), k2[pA], f2(cy.x, cy.y));
+            const float2 uB = __ffma2_rn(f2(X2, X2), k2[pB], f2(cy.z, cy.w));
+            const float2 dA0 = __ffma2_rn(uA, uA, f2(d2.x, d2.y));
+            const float2 dB0 = __ffma2_rn(uB, uB, f2(d2.z, d2.w));
+            const float2 nA = __ffma2_rn(uA, f2(pc.x, pc.y), f2(pc.x, pc.y));
+            const float2 nB = __ffma2_rn(uB, f2(pc.z, pc.w), f2(pc.z, pc.w));
+            const float2 dA = f2(q0 ? dA0.x : 1.0f, q1 ? dA0.y : 1.0f);
+            const float2 dB = f2(q2 ? dB0.x : 1.0f, q3 ? dB0.y : 1.0f);
+            const float2 q = __fmul2_rn(dA, dB);
+            const float2 rq = f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y));
+            const float2 iA = __fmul2_rn(dB, rq);
+            const float2 iB = __fmul2_rn(dA, rq);
+            acc[pA] = __ffma2_rn(nA, f2(q0 ? iA.x : 0.0f, q1 ? iA.y : 0.0f), acc[pA]);
+            acc[pB] = __ffma2_rn(nB, f2(q2 ? iB.x : 0.0f, q3 ? iB.y : 0.0f), acc[pB]);
+        };
 
         const int ngroups = split_groups(Lb - La, a.splits, split);
         auto gstart = [&](int gi) { return La + 32 * (split + gi * a.splits); };
@@ -1636,6 +1660,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             };
             // Partial lines away from every core: the window as a lane mask.
             auto masked_run = [&](int x, int y) {
+#pragma unroll 2
                 for (int t = x; t < y; ++t) {
                     const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
                     const bool in = jj >= SL[t].lo && jj < SL[t].hi && jj < t1;
@@ -1644,21 +1669,38 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                 }
             };
             // Core candidates: region I outside each condition's interval.
+            // The intervals are read from memory (core candidates are a small
+            // share of the lines), the next line's while this one is
+            // evaluated.
             auto cand_run = [&](int x, int y) {
+                LineIv<C> iv_next;
+                if (x < y) iv_next = ivl[gb + x];
                 for (int t = x; t < y; ++t) {
+                    const LineIv<C> iv = iv_next;
+                    if (t + 1 < y) iv_next = ivl[gb + t + 1];
                     const LineShX s = SL[t];
                     const bool full = (t >= a1 && t < d1);
                     const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
+                    if constexpr (NP % 2 == 0) {
+                        if (!(s.flags & (kLineWhole | kLineWide))) {
+                            // narrow: the shared reciprocal, a keep per condition
+                            const float X = fmaf(s.m - jf, s.dfn, s.rn);
+                            bool keep[C];
+#pragma unroll
+                            for (int c = 0; c < C; ++c) keep[c] = in && !(jj >= iv.lo[c] && jj <= iv.hi[c]);
+#pragma unroll
+                            for (int p = 0; p < NP; p += 2)
+                                region1_ab_keep(X * X, SR[t], p, p + 1, keep[2 * p], keep[2 * p + 1],
+                                                keep[2 * p + 2], keep[2 * p + 3]);
+                            continue;
+                        }
+                    }
                     // whole lines: X from the FP64 centre (rare; the grid
                     // value is read here rather than held for every line)
                     const float X = (s.flags & kLineWhole) ? float((s.nu - a.G.freq[jj < t1 ? jj : tl]) / s.nu)
                                             : fmaf(s.m - jf, s.dfn, s.rn);
                     const float X2 = X * X;
                     const float aX = fabsf(X);
-                    // the conditions' core intervals (the core pass's pairs),
-                    // read from memory: core candidates are a small share of
-                    // the lines
-                    const LineIv<C> iv = ivl[gb + t];
 #pragma unroll
                     for (int p = 0; p < NP; ++p) {
                         bool keep[2];

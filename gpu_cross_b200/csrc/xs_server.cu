@@ -273,6 +273,7 @@ struct Request {
     double* d_out = nullptr;
     size_t dev_bytes = 0, host_off = SIZE_MAX, host_bytes = 0;
     Clock::time_point t_submit, t_admit, t_done;
+    unsigned long long last_issue = 0;  // round robin: issue order of its last chunk
     int status = XS_OK;
     std::string error;
     bool done = false;
@@ -300,6 +301,7 @@ struct xs_server {
     size_t dev_requests = 0;    // grids + outputs of admitted requests
     std::vector<Molecule> mols;
     std::vector<Lane> lanes;
+    unsigned long long issue_seq = 0;  // chunks issued (round robin order)
     Arena arena;
     std::vector<cudaEvent_t> ev_pool;
 
@@ -554,13 +556,15 @@ void scheduler(xs_server* s) {
             int total = 0;
             for (const Lane& ln : s->lanes) total += int(ln.flight.size());
             const int cap = int(s->lanes.size());
+            const bool rr = s->cfg.policy == XS_POLICY_ROUND_ROBIN;
             while (total < cap) {
                 Request* best = nullptr;
                 for (Request* r : s->active)
                     if (r->next < r->chunks.size() && int(s->lanes[size_t(r->lane)].flight.size()) < depth &&
-                        (!best || r->remaining < best->remaining))
+                        (!best || (rr ? r->last_issue < best->last_issue : r->remaining < best->remaining)))
                         best = r;
                 if (!best) break;
+                best->last_issue = ++s->issue_seq;
                 if (!issue(s, best)) {
                     cudaGetLastError();
                     fail_all(s, std::string("launch failed: ") + xs_last_error());
@@ -621,6 +625,8 @@ int xs_server_create(int device, const xs_server_config* cfg, xs_server** out) {
     if (c.chunk_lines == 0) c.chunk_lines = size_t(1) << 22;
     if (c.host_budget == 0) c.host_budget = size_t(1) << 30;
     if (c.lanes > 16 || c.depth > 8) return sfail(XS_ERR_INVALID, "xs_server_create: lanes <= 16, depth <= 8");
+    if (c.policy != XS_POLICY_LEAST_WORK && c.policy != XS_POLICY_ROUND_ROBIN)
+        return sfail(XS_ERR_INVALID, "xs_server_create: unknown policy");
     auto* s = new xs_server();
     s->device = device;
     s->cfg = c;

@@ -368,7 +368,13 @@ typedef struct {
     int depth;            /* chunks in flight per lane (0 = 2) */
     double chunk_pairs;   /* target line-evals per chunk (0 = 4e9) */
     size_t chunk_lines;   /* most lines in one chunk's slice (0 = 2^22) */
+    int policy;           /* which admitted request's chunk goes next:
+                             XS_POLICY_LEAST_WORK (0, default): the one with
+                             the least remaining work; XS_POLICY_ROUND_ROBIN:
+                             each in turn (processor sharing by chunks) */
 } xs_server_config;
+#define XS_POLICY_LEAST_WORK 0
+#define XS_POLICY_ROUND_ROBIN 1
 
 typedef struct {
     int molecule;       /* id from xs_server_add_molecule */

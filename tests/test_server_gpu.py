@@ -81,9 +81,10 @@ def random_requests(mid, rng, k):
     return reqs
 
 
-def test_same_result_alone_and_in_a_mix(cuda, molecule):
+@pytest.mark.parametrize("policy", [capi.POLICY_LEAST_WORK, capi.POLICY_ROUND_ROBIN])
+def test_same_result_alone_and_in_a_mix(cuda, molecule, policy):
     rng = np.random.default_rng(77)
-    srv = capi.Server(0, lanes=4, depth=2, chunk_pairs=5e7)
+    srv = capi.Server(0, lanes=4, depth=2, chunk_pairs=5e7, policy=policy)
     try:
         mid = srv.add_molecule(molecule, MASS)
         reqs = random_requests(mid, rng, 24)
