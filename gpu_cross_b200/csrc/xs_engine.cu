@@ -640,7 +640,6 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         pa.cyp = reinterpret_cast<float2*>(base + plan.off_cyp);
         // window slots: groups with the same cut (consecutive) share the
         // first one's window data
-        pa.liv = reinterpret_cast<int*>(base + plan.off_liv);
         for (int g = 0; CG && g < nc / CG; ++g)
             pa.wslot[g] = (g > 0 && pa.cond[g * CG].cut == pa.cond[(g - 1) * CG].cut) ? pa.wslot[g - 1] : g;
 
@@ -682,7 +681,6 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         }
         if (CG) {
             sa.lsh = pa.lsh;
-            sa.liv = pa.liv;
             for (int g = 0; g < nc / CG; ++g) sa.wslot[g] = pa.wslot[g];
             sa.group = CG;
             sa.tiles_per_cond = (grid->points + 31) / 32;
@@ -731,6 +729,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
             ca.civ = pa.civ;
             ca.cyp = pa.cyp;
             ca.lsh = static_cast<const LineShX*>(pa.lsh);
+            ca.rec = pa.rec;
             ca.mi = pa.mi;
             ca.kc = pa.kc;
             ca.freq = G.freq;
@@ -744,6 +743,7 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
             ca.part_stride = sa.part_stride;
             for (int c = 0; c < nc; ++c) {
                 ca.kx[c] = sa.kx[c];
+                ca.kx2[c] = sa.kx2[c];
                 ca.row[c] = sa.row[c];
             }
             for (int g = 0; g < nc / CG; ++g) ca.wslot[g] = pa.wslot[g];

@@ -137,20 +137,16 @@ struct __align__(16) LineR1<2> {
 };
 static_assert(sizeof(LineR1<8>) == 96 && sizeof(LineR1<4>) == 48 && sizeof(LineR1<2>) == 32,
               "LineR1 layout");
-// The grid indices [lo, hi] of the chunk where the line's |x| + y < 15 (W4
-// regions II-IV; empty: lo > hi), per condition of the group: step two
-// leaves those pairs to the core pass.  Read from memory (not staged) by the
-// core-candidate lines only; line-major, so that one line's intervals are
-// one contiguous read.
-template <int C>
-struct __align__(16) LineIv {
-    int lo[C], hi[C];
-};
 // Bytes per (line, group) of the mixed multi-condition region-I records.
 constexpr size_t line_r1_bytes(int C) { return C == 8 ? 96 : (C == 4 ? 48 : 32); }
 // Per (line, condition) of the mixed multi-condition layout, for the core
 // pass: the grid indices of W4 regions II-IV [lo15, hi15] and III-IV
-// [lo55, hi55] (empty: lo > hi) inside the line's window.
+// [lo55, hi55] (empty: lo > hi) inside the line's window.  Step two adds
+// the region-I rational at every pair of the window except, on the lines it
+// takes as core candidates, the pairs where u = x^2 + y^2 - 0.5 < 1 in FP32
+// (near the centre the rational can exceed W4 by up to 0.28 / y); the core
+// pass makes the same choice and adds W4, less the rational where step two
+// added it, over [lo15, hi15].
 struct __align__(16) CoreIv {
     int lo15, hi15, lo55, hi55;
 };
@@ -206,7 +202,9 @@ struct PrepArgs {
     int* wlo;           // windows, condition-major
     int* whi;
     int* mi;            // nearest grid index of each line (condition-free)
-    int* kc;            // per condition: max core half-width in grid points;
+    int* kc;            // per condition: max core half-width in grid points
+                        // (mixed multi-condition layout: the core-candidate
+                        // reach plus one, 0 when no line has one);
                         // kc + kMaxCond: the core pass's reach (mixed
                         // multi-condition layout)
     unsigned* err;
@@ -225,7 +223,6 @@ struct PrepArgs {
     // copy of the per-line window data (LineShX / LineSh64, lo, hi), that of
     // the first group of their run.
     int wslot[kMaxCond];
-    int* liv;           // mixed multi-condition: LineIv<group> per (line, group)
     // Temperature classes: conditions of one class have the same cmcoef,
     // beta, Q, T_ref/T and Doppler width, so their intensity, Lorentz
     // temperature power and 1/Doppler width are the same numbers.  tclass[c]
@@ -249,7 +246,6 @@ struct StepArgs {
     size_t out_stride;  // elements between conditions
     GridDev G;
     const void* lsh;    // multi-condition layout (LineShX mixed, LineSh64 FP64)
-    const int* liv;     // mixed multi-condition: LineIv<group> per (line, group)
     int wslot[kMaxCond];  // window slot of each group (PrepArgs::wslot)
     int group;          // conditions per group (multi-condition kernel)
     int tiles_per_cond;
@@ -287,7 +283,7 @@ size_t record_bytes(int kind, bool mixed);
 // `ncond` conditions of `n` lines, the per-line grid index and the
 // per-condition core widths; sections 256-byte aligned from `base_off`.
 struct ScratchPlan {
-    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, off_liv, need;
+    size_t off_rec, off_wlo, off_whi, off_mi, off_kc, off_lsh, off_civ, off_cyp, need;
 };
 ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_off,
                          int group = 0);
@@ -299,6 +295,7 @@ struct CoreArgs {
     const CoreIv* civ;
     const float2* cyp;
     const LineShX* lsh;
+    const void* rec;    // LineR1<group> per (line, group): Cy of the condition
     const int* mi;
     const int* kc;
     const double* freq;
@@ -314,7 +311,8 @@ struct CoreArgs {
     int splits;
     double* part;
     size_t part_stride;
-    float kx[kMaxCond];  // 1 / dpw
+    float kx[kMaxCond];   // 1 / dpw
+    float kx2[kMaxCond];  // (1 / dpw)^2 as step two has it
     int row[kMaxCond];
     int wslot[kMaxCond];  // window slot of each group (PrepArgs::wslot)
 };

@@ -34,18 +34,22 @@ constexpr int kStages = 3;
 // per-pair path, x from its FP64 centre ("whole" lines): FP32 offsets and
 // the region-I sums are exact enough below it.
 constexpr double kWholeXMax = 1.0e8;
-// Scale of the shared-reciprocal products in region I (2^-100).  Region-I
-// denominators d = u^2 + 2 y^2 lie in [1.2e4, 1e32] (|x| + y >= 15, and
-// |x| < 1e8 for lines that are not whole), so tau d lies in [1e-26, 79],
-// tau dA dB in [1.2e-22, 7.9e33] and its reciprocal in [1.3e-34, 8e21]: all
-// normal FP32 numbers.
+// Scale of the shared-reciprocal products of the region-I rational (2^-100).
+// Where step two evaluates it (u >= 1), the denominators d = u^2 + 2 y^2
+// lie in [1, 1e32] (|x| < 1e8 for lines that are not whole), so tau d lies
+// in [7.9e-31, 79], tau dA dB in [7.9e-31, 7.9e33] and its reciprocal in
+// [1.3e-34, 1.3e30]: all normal FP32 numbers.
 constexpr float kPairTau = 7.88860905221011805e-31f;
-// Lines whose x^2 + y^2 stays below kPairUMax over their tiles for every
-// condition of the group ("narrow" lines, the usual case) share reciprocals
-// without the scaling: their region-I denominators d = u^2 + 2 y^2 lie in
-// [1.2e4, 6.3e18], so dA dB lies in [1.5e8, 4e37] and its reciprocal is a
-// normal FP32 number.  Other lines are marked kLineWide.
+// Lines whose x^2 + y^2 stays below kPairUMax over their tiles and whose
+// |Pc| stays below kPairPcMax, for every condition of the group ("narrow"
+// lines, the usual case), share reciprocals without the scaling: their
+// denominators lie in [1, 6.3e18], so dA dB lies in [1, 4e37] and its
+// reciprocal is a normal FP32 number, and the numerators |Pc (u + 1)| stay
+// below 2.5e17, so the cross products nA dB of two lines stay below 1.6e36
+// (and, d being >= 1, never fall below |n|).  Other lines are marked
+// kLineWide.
 constexpr double kPairUMax = 2.5e9;
+constexpr double kPairPcMax = 1.0e8;
 
 
 // ---------------------------------------------------------------------------
@@ -144,6 +148,11 @@ __global__ void k_grid_check(GridDev g, unsigned* err) {
 // ---------------------------------------------------------------------------
 // Step one.
 // ---------------------------------------------------------------------------
+// Mixed multi-condition layout: outside x^2 + y^2 < kNearR2 the region-I
+// rational stays below 2 Pc (u >= 1), so step two adds it there on every
+// line; inside, only the lines within the core-candidate reach can have
+// pairs, and step two tests u on them.
+constexpr double kNearR2 = 1.5;
 // Returns the line's core half-width in grid points (Voigt; 0 otherwise).
 // Grid indices [jlo, jhi] of the window [lo, hi) where |x| + y < lim, with
 // x = (nu - f_j) g in FP64 on the analytic grid f_j = f0 + j df: the region
@@ -456,8 +465,11 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
 // groups; the conditions follow in order, their loop not unrolled, which
 // keeps the code small.  Each value takes the FP64 path's operations in the
 // same order (the W4 region intervals are the FP64 region choice).  A
-// line's records of a group (LineR1, LineIv) are written by one thread
-// within a short time, so whole sectors reach memory.
+// line's LineR1 of a group is written by one thread within a short time, so
+// whole sectors reach memory.  The core-candidate reach (kc) covers the
+// pairs where x^2 + y^2 < kNearR2, at least one grid point beyond: there the
+// region-I rational may exceed W4 by far, and step two tests u on the lines
+// of that reach.
 template <int CONV, int C>
 __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
     static_assert(C % 2 == 0, "conditions come in pairs");
@@ -556,7 +568,6 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
         }
         const size_t gi = size_t(cg) * size_t(a.L.n) + size_t(live ? i : 0);
         LineR1<C>& lr = reinterpret_cast<LineR1<C>*>(a.rec)[gi];
-        LineIv<C>& li = reinterpret_cast<LineIv<C>*>(a.liv)[gi];
         if constexpr (C == 2) {
             if (live) lr.pad[0] = lr.pad[1] = 0.0f;
         }
@@ -582,7 +593,8 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                 const double Pc = pref * kW4C * y;
                 const double xw = (cut_prev + double(a.mixed_tile_span + 4) * df) * g;
                 const bool whole = far_m || !(xw < kWholeXMax);
-                wide = wide || !(xw * xw + y2 < kPairUMax);
+                // the shared reciprocals need the products in range
+                wide = wide || !(xw * xw + y2 < kPairUMax) || !(fabs(Pc) < kPairPcMax);
                 CoreIv iv;
                 const double q = nu_df * Cd.dpw;
                 region_interval_q(nu_p, g, y, 15.0, lo, hi, f0, df, md, q, iv.lo15, iv.hi15);
@@ -591,16 +603,17 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                     const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
                     rch = w < 3.0e7 ? int(w) : 30000000;
                     if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
+                    // |md - j| < sqrt(kNearR2 - y^2) q, |md - m| <= 1/2, one
+                    // point of margin, plus one (0: none)
+                    if (y2 < kNearR2) kcl = int(fmin(ceil(sqrt(kNearR2 - y2) * q + 0.5), 3.0e7)) + 2;
                 }
-                kcl = whole ? 30000000 : rch;  // a whole line is a core candidate of every tile
+                if (whole) kcl = 30000000;  // a core candidate of every tile
                 const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
                 a.civ[ci] = iv;
                 a.cyp[ci] = make_float2(float(y), float(pref));
                 lr.Cy[k] = float(y2 - 0.5);
                 lr.D2[k] = float(2.0 * y2);
                 lr.Pc[k] = float(Pc);
-                li.lo[k] = iv.lo15;
-                li.hi[k] = iv.hi15;
             }
             kcl = __reduce_max_sync(0xffffffffu, kcl);
             rch = __reduce_max_sync(0xffffffffu, rch);
@@ -764,6 +777,15 @@ __device__ __forceinline__ R w4_region2_re(R x, R y) {
     const R di = ui * (R(3) + R(2) * ur);
     const R br = (a + b * y2 - R(3) * b * x2) * dr + R(2) * x2 * (R(3) + R(2) * ur) * (nr + R(2) * b * y2);
     return region_div(y * br, dr * dr + di * di);
+}
+
+// The region-I rational of W4 in FP32 per unit pref, as step two evaluates
+// it: kW4C y (u + 1) / (u^2 + 2 y^2), u = x^2 + y^2 - 0.5.  The core pass
+// takes it back off the pairs where step two added it.
+__device__ __forceinline__ float w4_region1_re_f32(float x, float y) {
+    const float y2 = y * y;
+    const float u = fmaf(x, x, y2 - 0.5f);
+    return region_div(float(kW4C) * y * (u + 1.0f), fmaf(u, u, 2.0f * y2));
 }
 
 // W4 region III in FP32 (there y >= 0.195|x| - 0.176, so Re w is not small
@@ -1456,8 +1478,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt_mc(StepArgs a) {
 // pairs, each pair one packed FP32x2 operation per step of the region-I
 // rational (u = X^2 k^2 + Cy, u^2 + D2, Pc (u + 1), accumulate), so a
 // region-I pair costs two FP32 operations and one reciprocal per condition
-// and about three issue slots in all.  The pairs inside a line's region
-// interval (|x| + y < 15, from step one) are left to k_core_mcx.
+// and about three issue slots in all.  The rational is added at every pair
+// of the window except, on core candidates, where u < 1; k_core_mcx adds W4
+// less the rational (where it was added) inside the W4 region intervals
+// (|x| + y < 15, from step one).
 // ---------------------------------------------------------------------------
 // Resident blocks per SM the mixed multi-condition kernel asks the compiler
 // to fit: 24 warps per SM (about 80 registers a thread), except 8 conditions
@@ -1507,11 +1531,16 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         const int fs = int(warp_lower_bound(La, Lb, lane, [&](long i) { return whi[i] >= t1; }));
         const int Cb = int(warp_lower_bound(La, Lb, lane, [&](long i) { return wlo[i] > t0; }));
         const int fe = Cb > fs ? Cb : fs;
-        const int E = int(warp_lower_bound(La, Lb, lane, [&](long i) { return mi[i] >= t0 - kc; }));
-        const int Fc = int(warp_lower_bound(E, Lb, lane, [&](long i) { return mi[i] > tl + kc; }));
+        // core candidates [E, Fc): the lines whose near-centre pairs may
+        // fall in the tile (kc: the group's widest reach plus one; 0: no
+        // line of the group has such pairs)
+        int E = La, Fc = La;
+        if (kc > 0) {
+            E = int(warp_lower_bound(La, Lb, lane, [&](long i) { return mi[i] >= t0 - (kc - 1); }));
+            Fc = int(warp_lower_bound(E, Lb, lane, [&](long i) { return mi[i] > tl + (kc - 1); }));
+        }
         const LineShX* lsh = reinterpret_cast<const LineShX*>(a.lsh) + wbase;
         const R1* r1 = reinterpret_cast<const R1*>(a.rec) + gbase;
-        const LineIv<C>* ivl = reinterpret_cast<const LineIv<C>*>(a.liv) + gbase;
 
         const int jj = t0 + lane;
         const float jf = float(jj);
@@ -1527,25 +1556,31 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         // acc += Pc (u + 1) / (u^2 + D2).  Pairs where `keep` is false add
         // exactly zero: the reciprocal is replaced by 0 (not multiplied by a
         // mask, so that an infinite reciprocal of a skipped pair never
-        // reaches the sum); with GUARD the product itself is selected, for
-        // lines whose u may overflow.
-        auto region1 = [&](auto guard, float X2, const R1& r, int p, bool keep0, bool keep1) {
+        // reaches the sum).  MODE 0: plain; 1: the product itself is selected,
+        // for lines whose u may overflow; 2: as 1, and a pair is kept only
+        // where u >= 1 (core candidates: the core pass takes u < 1).
+        auto region1 = [&](auto mode, float X2, const R1& r, int p, bool keep0, bool keep1) {
+            constexpr int MODE = decltype(mode)::value;
             const float2 cy = *reinterpret_cast<const float2*>(&r.Cy[2 * p]);
             const float2 d2 = *reinterpret_cast<const float2*>(&r.D2[2 * p]);
             const float2 pc = *reinterpret_cast<const float2*>(&r.Pc[2 * p]);
             const float2 u = __ffma2_rn(f2(X2, X2), k2[p], cy);
+            if constexpr (MODE == 2) {
+                keep0 = keep0 && !(u.x < 1.0f);
+                keep1 = keep1 && !(u.y < 1.0f);
+            }
             const float2 den = __ffma2_rn(u, u, d2);
             const float2 num = __ffma2_rn(u, pc, pc);
             const float2 rr = f2(keep0 ? rcp_approx_f32(den.x) : 0.0f, keep1 ? rcp_approx_f32(den.y) : 0.0f);
-            if constexpr (decltype(guard)::value) {
+            if constexpr (MODE >= 1) {
                 acc[p].x += keep0 ? num.x * rr.x : 0.0f;
                 acc[p].y += keep1 ? num.y * rr.y : 0.0f;
             } else {
                 acc[p] = __ffma2_rn(num, rr, acc[p]);
             }
         };
-        const std::false_type plain;
-        const std::true_type guarded;
+        const std::integral_constant<int, 0> plain;
+        const std::integral_constant<int, 2> guarded_near;
         // Region I of two pairs of conditions (A, B) with one reciprocal per
         // two line-evals: lane h of A and lane h of B share 1 / (dA dB), so
         // 1/dA = dB / (dA dB) and 1/dB = dA / (dA dB).  For narrow lines the
@@ -1579,17 +1614,19 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         };
         const std::true_type narrow;
         const std::false_type scaled;
-        // region1_ab for a narrow core-candidate line, each condition with its
-        // own keep: a condition's pair that is not kept (inside its core
-        // interval or outside the window) enters the shared product as 1 and
-        // adds exactly zero, so the kept ones keep their region-I ranges.
-        auto region1_ab_keep = [&](float X2, const R1& r, int pA, int pB, bool q0, bool q1, bool q2,
-                                   bool q3) {
+        // region1_ab for a narrow core-candidate line: a condition's pair is
+        // kept where the point takes the line (`in`) and u >= 1 (the core
+        // pass takes u < 1); a pair that is not kept enters the shared
+        // product as 1 and adds exactly zero, so the kept ones keep their
+        // ranges.
+        auto region1_ab_near = [&](float X2, const R1& r, int pA, int pB, bool in) {
             const float4 cy = *reinterpret_cast<const float4*>(&r.Cy[2 * pA]);
             const float4 d2 = *reinterpret_cast<const float4*>(&r.D2[2 * pA]);
             const float4 pc = *reinterpret_cast<const float4*>(&r.Pc[2 * pA]);
             const float2 uA = __ffma2_rn(f2(X2, X2), k2[pA], f2(cy.x, cy.y));
             const float2 uB = __ffma2_rn(f2(X2, X2), k2[pB], f2(cy.z, cy.w));
+            const bool q0 = in && !(uA.x < 1.0f), q1 = in && !(uA.y < 1.0f);
+            const bool q2 = in && !(uB.x < 1.0f), q3 = in && !(uB.y < 1.0f);
             const float2 dA0 = __ffma2_rn(uA, uA, f2(d2.x, d2.y));
             const float2 dB0 = __ffma2_rn(uB, uB, f2(d2.z, d2.w));
             const float2 nA = __ffma2_rn(uA, f2(pc.x, pc.y), f2(pc.x, pc.y));
@@ -1650,48 +1687,81 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                 }
             };
             // Full lines away from every core: region I with no test.
-            auto fast_run = [&](int x, int y) {
-#pragma unroll 2
-                for (int t = x; t < y; ++t) {
-                    const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
-                    const float X = fmaf(s.x - jf, s.y, s.z);
-                    line_region1(X * X, SR[t], (__float_as_int(s.w) & kLineWide) != 0, true);
+            // Two narrow lines A, B that are not core candidates, at once: per
+            // condition one reciprocal for both lines, acc += (nA dB + nB dA)
+            // / (dA dB) (u >= 1 on such lines, so dA, dB >= 1; narrow lines
+            // keep dA dB and the products with Pc in range, kPairUMax).  inA,
+            // inB: the point takes the line (a line left out adds exactly 0).
+            auto pair_region1 = [&](float XA2, float XB2, const R1& ra, const R1& rb, bool inA, bool inB) {
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    const float2 cyA = *reinterpret_cast<const float2*>(&ra.Cy[2 * p]);
+                    const float2 d2A = *reinterpret_cast<const float2*>(&ra.D2[2 * p]);
+                    const float2 pcA = *reinterpret_cast<const float2*>(&ra.Pc[2 * p]);
+                    const float2 cyB = *reinterpret_cast<const float2*>(&rb.Cy[2 * p]);
+                    const float2 d2B = *reinterpret_cast<const float2*>(&rb.D2[2 * p]);
+                    const float2 pcB = *reinterpret_cast<const float2*>(&rb.Pc[2 * p]);
+                    const float2 uA = __ffma2_rn(f2(XA2, XA2), k2[p], cyA);
+                    const float2 uB = __ffma2_rn(f2(XB2, XB2), k2[p], cyB);
+                    const float2 dA = __ffma2_rn(uA, uA, d2A);
+                    const float2 dB = __ffma2_rn(uB, uB, d2B);
+                    float2 nA = __ffma2_rn(uA, pcA, pcA);
+                    float2 nB = __ffma2_rn(uB, pcB, pcB);
+                    if (!inA) nA = f2(0.0f, 0.0f);
+                    if (!inB) nB = f2(0.0f, 0.0f);
+                    const float2 q = __fmul2_rn(dA, dB);
+                    const float2 sn = __ffma2_rn(nB, dA, __fmul2_rn(nA, dB));
+                    acc[p] = __ffma2_rn(sn, f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)), acc[p]);
                 }
             };
+            // Lines [x, y) that are not core candidates, two at a time; `full`:
+            // their windows cover the tile, else the window is a lane mask.
+            auto pair_run = [&](int x, int y, auto full) {
+                auto in_of = [&](int t) {
+                    if constexpr (decltype(full)::value) return true;
+                    else return jj >= SL[t].lo && jj < SL[t].hi && jj < t1;
+                };
+                int t = x;
+                for (; t + 1 < y; t += 2) {
+                    const float4 sA = *reinterpret_cast<const float4*>(&SL[t]);
+                    const float4 sB = *reinterpret_cast<const float4*>(&SL[t + 1]);
+                    const float XA = fmaf(sA.x - jf, sA.y, sA.z);
+                    const float XB = fmaf(sB.x - jf, sB.y, sB.z);
+                    const int fA = __float_as_int(sA.w), fB = __float_as_int(sB.w);
+                    const bool inA = in_of(t), inB = in_of(t + 1);
+                    if (!((fA | fB) & kLineWide)) {
+                        pair_region1(XA * XA, XB * XB, SR[t], SR[t + 1], inA, inB);
+                    } else {
+                        line_region1(XA * XA, SR[t], (fA & kLineWide) != 0, inA);
+                        line_region1(XB * XB, SR[t + 1], (fB & kLineWide) != 0, inB);
+                    }
+                }
+                if (t < y) {
+                    const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
+                    const float X = fmaf(s.x - jf, s.y, s.z);
+                    line_region1(X * X, SR[t], (__float_as_int(s.w) & kLineWide) != 0, in_of(t));
+                }
+            };
+            const std::true_type full_lines;
+            const std::false_type partial_lines;
+            // Full lines away from every core: region I with no test.
+            auto fast_run = [&](int x, int y) { pair_run(x, y, full_lines); };
             // Partial lines away from every core: the window as a lane mask.
-            auto masked_run = [&](int x, int y) {
-#pragma unroll 2
-                for (int t = x; t < y; ++t) {
-                    const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
-                    const bool in = jj >= SL[t].lo && jj < SL[t].hi && jj < t1;
-                    const float X = fmaf(s.x - jf, s.y, s.z);
-                    line_region1(X * X, SR[t], (__float_as_int(s.w) & kLineWide) != 0, in);
-                }
-            };
-            // Core candidates: region I outside each condition's interval.
-            // The intervals are read from memory (core candidates are a small
-            // share of the lines), the next line's while this one is
-            // evaluated.
+            auto masked_run = [&](int x, int y) { pair_run(x, y, partial_lines); };
+            // Core candidates: region I where u >= 1, per condition (the
+            // core pass takes the pairs with u < 1, deciding on the same FP32
+            // u).
             auto cand_run = [&](int x, int y) {
-                LineIv<C> iv_next;
-                if (x < y) iv_next = ivl[gb + x];
                 for (int t = x; t < y; ++t) {
-                    const LineIv<C> iv = iv_next;
-                    if (t + 1 < y) iv_next = ivl[gb + t + 1];
                     const LineShX s = SL[t];
                     const bool full = (t >= a1 && t < d1);
                     const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
                     if constexpr (NP % 2 == 0) {
                         if (!(s.flags & (kLineWhole | kLineWide))) {
-                            // narrow: the shared reciprocal, a keep per condition
+                            // narrow: the shared reciprocal
                             const float X = fmaf(s.m - jf, s.dfn, s.rn);
-                            bool keep[C];
 #pragma unroll
-                            for (int c = 0; c < C; ++c) keep[c] = in && !(jj >= iv.lo[c] && jj <= iv.hi[c]);
-#pragma unroll
-                            for (int p = 0; p < NP; p += 2)
-                                region1_ab_keep(X * X, SR[t], p, p + 1, keep[2 * p], keep[2 * p + 1],
-                                                keep[2 * p + 2], keep[2 * p + 3]);
+                            for (int p = 0; p < NP; p += 2) region1_ab_near(X * X, SR[t], p, p + 1, in);
                             continue;
                         }
                     }
@@ -1709,10 +1779,9 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                             const int c = 2 * p + h;
                             // beyond x ~ 1e9 (lines far off the FP32 offset
                             // range) region I is taken as 0
-                            keep[h] = in && !(jj >= iv.lo[c] && jj <= iv.hi[c]) &&
-                                      aX * a.kx[cg * C + c] < 1.0e9f;
+                            keep[h] = in && aX * a.kx[cg * C + c] < 1.0e9f;
                         }
-                        region1(guarded, X2, SR[t], p, keep[0], keep[1]);
+                        region1(guarded_near, X2, SR[t], p, keep[0], keep[1]);
                     }
                 }
             };
@@ -1760,7 +1829,7 @@ __device__ __forceinline__ void core_table_clear(float (*T)[kCoreRow], int lane)
     __syncwarp();
 }
 // Sum of this lane's row in line order.  Entries of lines that wrote nothing
-// are +0 and leave the (non-negative) sum unchanged.
+// are +0.
 __device__ __forceinline__ float core_table_column(float (*T)[kCoreRow], int lane) {
     float part = 0.0f;
 #pragma unroll
@@ -1780,8 +1849,9 @@ __device__ __forceinline__ float core_table_column(float (*T)[kCoreRow], int lan
 // widest interval bounds the reach), taken 32 at a time: each lane evaluates
 // W4 regions II-IV (region III-IV interval from step one, region III or IV
 // by Humlicek's test on the FP32 x, y) at the row's points inside its line's
-// interval and writes them to a per-warp table, then each lane adds its
-// point's column in line order.  Sums are FP32 per batch of 32 lines and FP64
+// interval, less the region-I rational where step two added it, and writes
+// them to a per-warp table, then each lane adds its point's column in line
+// order.  Sums are FP32 per batch of 32 lines and FP64
 // across batches, in a fixed order.  With line splits (blockIdx.z = split) a
 // row's batches are shared out as in step two and the sums go to the parts.
 template <int WARPS>
@@ -1800,10 +1870,18 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     const int K = a.kc[kMaxCond + c];  // the condition's core-pass reach
     const long E = warp_lower_bound(0, a.n, lane, [&](long i) { return a.mi[i] >= t0 - K; });
     const long F = warp_lower_bound(E, a.n, lane, [&](long i) { return a.mi[i] > tl + K; });
+    const int g = c / a.group, kg = c - g * a.group;
     const CoreIv* civ = a.civ + size_t(c) * size_t(a.n);
     const float2* cyp = a.cyp + size_t(c) * size_t(a.n);
-    const LineShX* lsh = a.lsh + size_t(a.wslot[c / a.group]) * size_t(a.n);
-    const float k = a.kx[c];
+    const LineShX* lsh = a.lsh + size_t(a.wslot[g]) * size_t(a.n);
+    // Cy of this condition in the group's LineR1 records (step two's u)
+    const size_t r1b = line_r1_bytes(a.group);
+    const unsigned char* r1 = static_cast<const unsigned char*>(a.rec) + size_t(g) * size_t(a.n) * r1b +
+                              sizeof(float) * size_t(kg);
+    // step two's core candidates of this row: the group's reach (kc - 1)
+    int kcg = 0;
+    for (int q = 0; q < a.group; ++q) kcg = max(kcg, a.kc[g * a.group + q]);
+    const float k = a.kx[c], k2 = a.kx2[c];
     const int split = int(blockIdx.z), S = a.splits;
     double acc = 0.0;
     for (long b = E + 32L * split; b < F; b += 32L * S) {
@@ -1816,6 +1894,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
             if (jlo <= jhi) {
                 const LineShX s = lsh[i];
                 const float2 yp = cyp[i];
+                const int mline = a.mi[i];
+                const bool cand = kcg > 0 && mline >= t0 - (kcg - 1) && mline <= tl + (kcg - 1);
+                const float cy = cand ? *reinterpret_cast<const float*>(r1 + size_t(i) * r1b) : 0.0f;
                 for (int j = jlo; j <= jhi; ++j) {
                     const float X = (s.flags & kLineWhole) ? float((s.nu - a.freq[j]) / s.nu)
                                                            : fmaf(s.m - float(j), s.dfn, s.rn);
@@ -1825,6 +1906,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
                         w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y) : w4_region4_re_f32(ax, y);
                     else
                         w = w4_region2_re<float>(ax, y);
+                    // step two added the region-I rational here unless the
+                    // line was its core candidate and u < 1 (the same FP32 u)
+                    if (!(cand && fmaf(X * X, k2, cy) < 1.0f)) w -= w4_region1_re_f32(ax, y);
                     T[j - t0][lane] = yp.y * w;
                 }
             }
@@ -2389,8 +2473,7 @@ ScratchPlan plan_scratch(int kind, bool mixed, size_t n, int ncond, size_t base_
     p.off_civ = al(p.off_lsh + (group > 0 ? lsh * n * nwin : 0));
     const bool core = mixed && group > 0;
     p.off_cyp = al(p.off_civ + (core ? sizeof(CoreIv) * n * size_t(ncond) : 0));
-    p.off_liv = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
-    p.need = al(p.off_liv + (core ? 2 * sizeof(int) * size_t(group) * n * nwin : 0));
+    p.need = al(p.off_cyp + (core ? sizeof(float2) * n * size_t(ncond) : 0));
     return p;
 }
 
