@@ -1692,26 +1692,45 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             // / (dA dB) (u >= 1 on such lines, so dA, dB >= 1; narrow lines
             // keep dA dB and the products with Pc in range, kPairUMax).  inA,
             // inB: the point takes the line (a line left out adds exactly 0).
+            auto pair_step = [&](float XA2, float XB2, float2 cyA, float2 d2A, float2 pcA, float2 cyB,
+                                 float2 d2B, float2 pcB, int p, bool inA, bool inB) {
+                const float2 uA = __ffma2_rn(f2(XA2, XA2), k2[p], cyA);
+                const float2 uB = __ffma2_rn(f2(XB2, XB2), k2[p], cyB);
+                const float2 dA = __ffma2_rn(uA, uA, d2A);
+                const float2 dB = __ffma2_rn(uB, uB, d2B);
+                float2 nA = __ffma2_rn(uA, pcA, pcA);
+                float2 nB = __ffma2_rn(uB, pcB, pcB);
+                if (!inA) nA = f2(0.0f, 0.0f);
+                if (!inB) nB = f2(0.0f, 0.0f);
+                const float2 q = __fmul2_rn(dA, dB);
+                const float2 sn = __ffma2_rn(nB, dA, __fmul2_rn(nA, dB));
+                acc[p] = __ffma2_rn(sn, f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)), acc[p]);
+            };
             auto pair_region1 = [&](float XA2, float XB2, const R1& ra, const R1& rb, bool inA, bool inB) {
+                if constexpr (NP % 2 == 0) {
+                    // conditions 4q..4q+3: one 16-byte load per array and line
 #pragma unroll
-                for (int p = 0; p < NP; ++p) {
-                    const float2 cyA = *reinterpret_cast<const float2*>(&ra.Cy[2 * p]);
-                    const float2 d2A = *reinterpret_cast<const float2*>(&ra.D2[2 * p]);
-                    const float2 pcA = *reinterpret_cast<const float2*>(&ra.Pc[2 * p]);
-                    const float2 cyB = *reinterpret_cast<const float2*>(&rb.Cy[2 * p]);
-                    const float2 d2B = *reinterpret_cast<const float2*>(&rb.D2[2 * p]);
-                    const float2 pcB = *reinterpret_cast<const float2*>(&rb.Pc[2 * p]);
-                    const float2 uA = __ffma2_rn(f2(XA2, XA2), k2[p], cyA);
-                    const float2 uB = __ffma2_rn(f2(XB2, XB2), k2[p], cyB);
-                    const float2 dA = __ffma2_rn(uA, uA, d2A);
-                    const float2 dB = __ffma2_rn(uB, uB, d2B);
-                    float2 nA = __ffma2_rn(uA, pcA, pcA);
-                    float2 nB = __ffma2_rn(uB, pcB, pcB);
-                    if (!inA) nA = f2(0.0f, 0.0f);
-                    if (!inB) nB = f2(0.0f, 0.0f);
-                    const float2 q = __fmul2_rn(dA, dB);
-                    const float2 sn = __ffma2_rn(nB, dA, __fmul2_rn(nA, dB));
-                    acc[p] = __ffma2_rn(sn, f2(rcp_approx_f32(q.x), rcp_approx_f32(q.y)), acc[p]);
+                    for (int p = 0; p < NP; p += 2) {
+                        const float4 cyA = *reinterpret_cast<const float4*>(&ra.Cy[2 * p]);
+                        const float4 d2A = *reinterpret_cast<const float4*>(&ra.D2[2 * p]);
+                        const float4 pcA = *reinterpret_cast<const float4*>(&ra.Pc[2 * p]);
+                        const float4 cyB = *reinterpret_cast<const float4*>(&rb.Cy[2 * p]);
+                        const float4 d2B = *reinterpret_cast<const float4*>(&rb.D2[2 * p]);
+                        const float4 pcB = *reinterpret_cast<const float4*>(&rb.Pc[2 * p]);
+                        pair_step(XA2, XB2, f2(cyA.x, cyA.y), f2(d2A.x, d2A.y), f2(pcA.x, pcA.y), f2(cyB.x, cyB.y),
+                                  f2(d2B.x, d2B.y), f2(pcB.x, pcB.y), p, inA, inB);
+                        pair_step(XA2, XB2, f2(cyA.z, cyA.w), f2(d2A.z, d2A.w), f2(pcA.z, pcA.w), f2(cyB.z, cyB.w),
+                                  f2(d2B.z, d2B.w), f2(pcB.z, pcB.w), p + 1, inA, inB);
+                    }
+                } else {
+#pragma unroll
+                    for (int p = 0; p < NP; ++p)
+                        pair_step(XA2, XB2, *reinterpret_cast<const float2*>(&ra.Cy[2 * p]),
+                                  *reinterpret_cast<const float2*>(&ra.D2[2 * p]),
+                                  *reinterpret_cast<const float2*>(&ra.Pc[2 * p]),
+                                  *reinterpret_cast<const float2*>(&rb.Cy[2 * p]),
+                                  *reinterpret_cast<const float2*>(&rb.D2[2 * p]),
+                                  *reinterpret_cast<const float2*>(&rb.Pc[2 * p]), p, inA, inB);
                 }
             };
             // Lines [x, y) that are not core candidates, two at a time; `full`:
@@ -1859,17 +1878,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     __shared__ __align__(16) float tab[WARPS][32][kCoreRow];  // [point][line of the batch]
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int c = int(blockIdx.y);
-    const int t0 = a.G.start + (int(blockIdx.x) * WARPS + warp) * 32;
+    // blockIdx.x = condition, so that the blocks of one set of rows run
+    // together and the lines' shared data (LineShX, mi) comes from DRAM once
+    // for all conditions; blockIdx.y steps over the sets of WARPS rows.
+    const int c = int(blockIdx.x);
     const int end = a.G.start + a.G.points;
-    if (t0 >= end) return;
+    const int row_sets = (a.G.points + 32 * WARPS - 1) / (32 * WARPS);
     float (*T)[kCoreRow] = tab[warp];
     core_table_clear(T, lane);
-    const int t1 = t0 + 32 < end ? t0 + 32 : end;
-    const int tl = t1 - 1;
     const int K = a.kc[kMaxCond + c];  // the condition's core-pass reach
-    const long E = warp_lower_bound(0, a.n, lane, [&](long i) { return a.mi[i] >= t0 - K; });
-    const long F = warp_lower_bound(E, a.n, lane, [&](long i) { return a.mi[i] > tl + K; });
     const int g = c / a.group, kg = c - g * a.group;
     const CoreIv* civ = a.civ + size_t(c) * size_t(a.n);
     const float2* cyp = a.cyp + size_t(c) * size_t(a.n);
@@ -1878,52 +1895,61 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
     const size_t r1b = line_r1_bytes(a.group);
     const unsigned char* r1 = static_cast<const unsigned char*>(a.rec) + size_t(g) * size_t(a.n) * r1b +
                               sizeof(float) * size_t(kg);
-    // step two's core candidates of this row: the group's reach (kc - 1)
+    // step two's core candidates of a row: the group's reach (kc - 1)
     int kcg = 0;
     for (int q = 0; q < a.group; ++q) kcg = max(kcg, a.kc[g * a.group + q]);
     const float k = a.kx[c], k2 = a.kx2[c];
     const int split = int(blockIdx.z), S = a.splits;
-    double acc = 0.0;
-    for (long b = E + 32L * split; b < F; b += 32L * S) {
-        const long i = b + lane;
-        int jlo = 1, jhi = 0;
-        if (i < F) {
-            const CoreIv iv = civ[i];
-            jlo = max(iv.lo15, t0);
-            jhi = min(iv.hi15, tl);
-            if (jlo <= jhi) {
-                const LineShX s = lsh[i];
-                const float2 yp = cyp[i];
-                const int mline = a.mi[i];
-                const bool cand = kcg > 0 && mline >= t0 - (kcg - 1) && mline <= tl + (kcg - 1);
-                const float cy = cand ? *reinterpret_cast<const float*>(r1 + size_t(i) * r1b) : 0.0f;
-                for (int j = jlo; j <= jhi; ++j) {
-                    const float X = (s.flags & kLineWhole) ? float((s.nu - a.freq[j]) / s.nu)
-                                                           : fmaf(s.m - float(j), s.dfn, s.rn);
-                    const float ax = fabsf(X) * k, y = yp.x;
-                    float w;
-                    if (j >= iv.lo55 && j <= iv.hi55)
-                        w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y) : w4_region4_re_f32(ax, y);
-                    else
-                        w = w4_region2_re<float>(ax, y);
-                    // step two added the region-I rational here unless the
-                    // line was its core candidate and u < 1 (the same FP32 u)
-                    if (!(cand && fmaf(X * X, k2, cy) < 1.0f)) w -= w4_region1_re_f32(ax, y);
-                    T[j - t0][lane] = yp.y * w;
+    for (int rs = int(blockIdx.y); rs < row_sets; rs += int(gridDim.y)) {
+        const int t0 = a.G.start + (rs * WARPS + warp) * 32;
+        if (t0 >= end) break;  // warp-uniform; later sets start further on
+        const int t1 = t0 + 32 < end ? t0 + 32 : end;
+        const int tl = t1 - 1;
+        const long E = warp_lower_bound(0, a.n, lane, [&](long i) { return a.mi[i] >= t0 - K; });
+        const long F = warp_lower_bound(E, a.n, lane, [&](long i) { return a.mi[i] > tl + K; });
+        double acc = 0.0;
+        for (long b = E + 32L * split; b < F; b += 32L * S) {
+            const long i = b + lane;
+            int jlo = 1, jhi = 0;
+            if (i < F) {
+                const CoreIv iv = civ[i];
+                jlo = max(iv.lo15, t0);
+                jhi = min(iv.hi15, tl);
+                if (jlo <= jhi) {
+                    const LineShX s = lsh[i];
+                    const float2 yp = cyp[i];
+                    const int mline = a.mi[i];
+                    const bool cand = kcg > 0 && mline >= t0 - (kcg - 1) && mline <= tl + (kcg - 1);
+                    const float cy = cand ? *reinterpret_cast<const float*>(r1 + size_t(i) * r1b) : 0.0f;
+                    for (int j = jlo; j <= jhi; ++j) {
+                        const float X = (s.flags & kLineWhole) ? float((s.nu - a.freq[j]) / s.nu)
+                                                               : fmaf(s.m - float(j), s.dfn, s.rn);
+                        const float ax = fabsf(X) * k, y = yp.x;
+                        float w;
+                        if (j >= iv.lo55 && j <= iv.hi55)
+                            w = (y >= fmaf(0.195f, ax, -0.176f)) ? w4_region3_re_f32(ax, y)
+                                                                  : w4_region4_re_f32(ax, y);
+                        else
+                            w = w4_region2_re<float>(ax, y);
+                        // step two added the region-I rational here unless the
+                        // line was its core candidate and u < 1 (the same FP32 u)
+                        if (!(cand && fmaf(X * X, k2, cy) < 1.0f)) w -= w4_region1_re_f32(ax, y);
+                        T[j - t0][lane] = yp.y * w;
+                    }
                 }
             }
+            __syncwarp();
+            acc += double(core_table_column(T, lane));
+            __syncwarp();
+            for (int j = jlo; j <= jhi; ++j) T[j - t0][lane] = 0.0f;  // back to all zeros
         }
-        __syncwarp();
-        acc += double(core_table_column(T, lane));
-        __syncwarp();
-        for (int j = jlo; j <= jhi; ++j) T[j - t0][lane] = 0.0f;  // back to all zeros
-    }
-    const int jj = t0 + lane;
-    if (jj < t1) {
-        if (S <= 1)
-            a.out[size_t(a.row[c]) * a.out_stride + size_t(jj)] += acc;
-        else
-            a.part[(size_t(c) * S + split) * a.part_stride + size_t(jj - a.G.start)] += acc;
+        const int jj = t0 + lane;
+        if (jj < t1) {
+            if (S <= 1)
+                a.out[size_t(a.row[c]) * a.out_stride + size_t(jj)] += acc;
+            else
+                a.part[(size_t(c) * S + split) * a.part_stride + size_t(jj - a.G.start)] += acc;
+        }
     }
 }
 
@@ -2432,7 +2458,8 @@ cudaError_t launch_core_mcx(const CoreArgs& a, int ncond, cudaStream_t stream) {
     constexpr int W = 4;
     const int rows = (a.G.points + 31) / 32;
     const unsigned S = unsigned(a.splits > 1 ? a.splits : 1);
-    k_core_mcx<W><<<dim3(unsigned((rows + W - 1) / W), unsigned(ncond), S), W * 32, 0, stream>>>(a);
+    const int sets = (rows + W - 1) / W;
+    k_core_mcx<W><<<dim3(unsigned(ncond), unsigned(sets < 65535 ? sets : 65535), S), W * 32, 0, stream>>>(a);
     return cudaGetLastError();
 }
 
