@@ -605,7 +605,9 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                     if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
                     // |md - j| < sqrt(kNearR2 - y^2) q, |md - m| <= 1/2, one
                     // point of margin, plus one (0: none)
-                    if (y2 < kNearR2) kcl = int(fmin(ceil(sqrt(kNearR2 - y2) * q + 0.5), 3.0e7)) + 2;
+                    // (in FP32, widened by 1e-6 for its rounding)
+                    if (y2 < kNearR2)
+                        kcl = int(fminf(ceilf(sqrtf(float(kNearR2 - y2)) * float(q) * 1.000001f + 0.5f), 3.0e7f)) + 2;
                 }
                 if (whole) kcl = 30000000;  // a core candidate of every tile
                 const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
@@ -1848,9 +1850,14 @@ __device__ __forceinline__ void core_table_clear(float (*T)[kCoreRow], int lane)
     __syncwarp();
 }
 // Sum of this lane's row in line order.  Entries of lines that wrote nothing
-// are +0.
-__device__ __forceinline__ float core_table_column(float (*T)[kCoreRow], int lane) {
+// are +0, so adding only the columns of `written` (the lines that wrote
+// something; few in a sparse batch) gives the same sum.  Warp-uniform.
+__device__ __forceinline__ float core_table_column(float (*T)[kCoreRow], int lane, unsigned written) {
     float part = 0.0f;
+    if (__popc(written) <= 8) {
+        for (unsigned m = written; m != 0u; m &= m - 1u) part += T[lane][__ffs(m) - 1];
+        return part;
+    }
 #pragma unroll
     for (int q = 0; q < 32; q += 4) {
         const float4 v = *reinterpret_cast<const float4*>(&T[lane][q]);
@@ -1938,8 +1945,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_mcx(CoreArgs a) {
                     }
                 }
             }
+            const unsigned written = __ballot_sync(0xffffffffu, jlo <= jhi);
+            if (written == 0u) continue;  // no pair in this batch
             __syncwarp();
-            acc += double(core_table_column(T, lane));
+            acc += double(core_table_column(T, lane, written));
             __syncwarp();
             for (int j = jlo; j <= jhi; ++j) T[j - t0][lane] = 0.0f;  // back to all zeros
         }
@@ -1995,8 +2004,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_core_v32(StepArgs a) {
                 T[j - t0][lane] = r.pref * w;
             }
         }
+        const unsigned written = __ballot_sync(0xffffffffu, jlo <= jhi);
+        if (written == 0u) continue;  // no pair in this batch
         __syncwarp();
-        acc += double(core_table_column(T, lane));
+        acc += double(core_table_column(T, lane, written));
         __syncwarp();
         for (int j = jlo; j <= jhi; ++j) T[j - t0][lane] = 0.0f;  // back to all zeros
     }

@@ -200,12 +200,15 @@ int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* c
  * arithmetic of the same reference convention (no counterpart in the
  * reference, which computes in FP64 only).
  *   bound_rel: a-priori bound on the relative error of every grid point of
- *     the result, and so of the band integral (all terms are positive for
- *     non-negative intensities).  Mixed Voigt: 1024 * 2^-24 = 6.1e-5, twice
- *     the rounding-error analysis of the FP32 steps (region I: offset, u,
- *     u^2 + 2y^2, the shared reciprocal, 32-line FP32 partial sums folded
- *     with compensation; regions II-IV: the FP32 x and y through the
- *     profile's sensitivity, at most 2 x^2 = 60.5, and the FP32 W4 forms).
+ *     the result, and so of the band integral (every pair's true value is
+ *     positive for non-negative intensities).  Mixed Voigt: 1024 * 2^-24 =
+ *     6.1e-5, above the rounding-error analysis of the FP32 steps (region I:
+ *     offset, u, u^2 + 2y^2, the shared reciprocal, 32-line FP32 partial sums
+ *     folded with compensation, 76 * 2^-24; regions II-IV: the FP32 x and y
+ *     through the profile's sensitivity, at most 2 x^2 = 60.5, the FP32 W4
+ *     forms and, for several conditions at once, the region-I value that
+ *     step two adds there and the core pass takes back, at most 1.21 W4 --
+ *     about 690 * 2^-24).
  *     FP64 (every FP64 result, Doppler and Gaussian included): 1e-12,
  *     summation order only.
  *   sampled_*: with xs_options.check_rows > 0 (mixed Voigt), measured on
