@@ -70,7 +70,8 @@ class GridC(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device_budget", ctypes.c_size_t), ("host_budget", ctypes.c_size_t),
                 ("lanes", ctypes.c_int), ("depth", ctypes.c_int), ("chunk_pairs", ctypes.c_double),
-                ("chunk_lines", ctypes.c_size_t), ("policy", ctypes.c_int)]
+                ("chunk_lines", ctypes.c_size_t), ("policy", ctypes.c_int),
+                ("tcache_bytes", ctypes.c_longlong)]
 
 
 class Request(ctypes.Structure):
@@ -84,7 +85,7 @@ class RequestInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("latency_ms", ctypes.c_double),
                 ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("chunks", ctypes.c_int),
                 ("line_evals", ctypes.c_double), ("lines", ctypes.c_size_t),
-                ("err_bound", ctypes.c_double)]
+                ("err_bound", ctypes.c_double), ("tcache_chunks", ctypes.c_int)]
 
 
 class TuneResult(ctypes.Structure):
@@ -122,6 +123,9 @@ _SIGS = {
     "xs_scratch_bytes_needed": (_SZ, [ctypes.POINTER(Options), _I, _SZ]),
     "xs_engine_execute": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _I,
                                ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP, _SZ]),
+    "xs_engine_execute_host": (_I, [_VP, ctypes.POINTER(Options), ctypes.POINTER(Condition), _I,
+                                    ctypes.POINTER(Lines), ctypes.POINTER(Lines), ctypes.POINTER(GridC), _VP,
+                                    _SZ, _VP, _I]),
     "xs_engine_last_stats": (_I, [_VP, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "xs_engine_accuracy": (_I, [_VP, _VP]),
     "xs_error_bound": (_D, [_I, _I]),
@@ -252,6 +256,17 @@ class Engine:
         arr = (Condition * len(conds))(*conds)
         check(lib().xs_engine_execute(self.h, ctypes.byref(opts), arr, len(conds),
                                       ctypes.byref(lines), ctypes.byref(grid), out_ptr, out_stride))
+
+    def execute_host(self, opts: Options, conds: list[Condition], host_lines: Lines, dev_lines: Lines,
+                     grid: GridC, out_ptr: int, out_stride: int = 0, host_out_ptr: int | None = None,
+                     pieces: int = 8) -> None:
+        """xs_engine_execute_host: lines from (pinned) host arrays, copied in
+        `pieces` slices that overlap step one; the result span copied to
+        host_out_ptr.  Asynchronous: sync() before reading it."""
+        arr = (Condition * len(conds))(*conds)
+        check(lib().xs_engine_execute_host(self.h, ctypes.byref(opts), arr, len(conds),
+                                           ctypes.byref(host_lines), ctypes.byref(dev_lines),
+                                           ctypes.byref(grid), out_ptr, out_stride, host_out_ptr, pieces))
 
     def accuracy(self) -> dict:
         """xs_engine_accuracy: the error statement of the last execute."""
@@ -457,8 +472,9 @@ class Server:
 
     def __init__(self, device: int = 0, device_budget: int = 0, host_budget: int = 0,
                  lanes: int = 0, depth: int = 0, chunk_pairs: float = 0.0, chunk_lines: int = 0,
-                 policy: int = 0):
-        cfg = ServerConfig(device_budget, host_budget, lanes, depth, chunk_pairs, chunk_lines, policy)
+                 policy: int = 0, tcache_bytes: int = 0):
+        cfg = ServerConfig(device_budget, host_budget, lanes, depth, chunk_pairs, chunk_lines, policy,
+                           tcache_bytes)
         h = ctypes.c_void_p()
         check(lib().xs_server_create(device, ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h

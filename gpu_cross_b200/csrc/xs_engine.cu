@@ -45,6 +45,9 @@ int cuda_fail(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
+// Most slices of a host line list (xs_engine_execute_host).
+constexpr int kMaxPieces = 16;
+
 // Restores the caller's current device on scope exit.
 struct DeviceGuard {
     int prev = -1;
@@ -69,6 +72,10 @@ struct xs_engine {
     unsigned* d_words = nullptr;  // [0] error bits, [1] work counter
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     bool timed = false;
+    // host line lists (xs_engine_execute_host): a copy stream and an event
+    // per slice, made on first use
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pev[kMaxPieces + 1] = {};
     // error statement of the last execute: the a-priori bound and, with
     // sampled rows, where their statistics are ([c][4] doubles)
     double bound_rel = 0.0;
@@ -245,6 +252,9 @@ int xs_engine_destroy(xs_engine* e) {
         else cudaDeviceSynchronize();
         for (auto& ev : e->ev)
             if (ev) cudaEventDestroy(ev);
+        for (auto& ev : e->pev)
+            if (ev) cudaEventDestroy(ev);
+        if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
         cudaFree(e->scratch);
         cudaFree(e->d_words);
     }
@@ -297,6 +307,37 @@ size_t xs_scratch_bytes_needed(const xs_options* opt, int ncond, size_t n_lines)
 int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
                       const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride) {
     return xs::engine_execute(e, opt, conds, ncond, lines, grid, out, out_stride, nullptr);
+}
+
+int xs_engine_execute_host(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                           const xs_lines* host_lines, const xs_lines* dev_lines, const xs_grid* grid,
+                           double* out, size_t out_stride, double* host_out, int pieces) {
+    if (!e || !host_lines || !dev_lines || !grid)
+        return fail(XS_ERR_INVALID, "xs_engine_execute_host: NULL argument");
+    if (host_lines->count != dev_lines->count)
+        return fail(XS_ERR_INVALID, "xs_engine_execute_host: host and device line counts differ");
+    if (!host_lines->nu || !host_lines->energies || !host_lines->aif || !host_lines->gns)
+        return fail(XS_ERR_INVALID, "xs_engine_execute_host: host line arrays missing");
+    if (opt && opt->profile == XS_VOIGT && (!host_lines->gamma || !host_lines->n))
+        return fail(XS_ERR_INVALID, "xs_engine_execute_host: VOIGT needs gamma and n");
+    if (pieces < 1 || pieces > kMaxPieces)
+        return fail(XS_ERR_INVALID, "xs_engine_execute_host: pieces must be 1..16");
+    xs::ExecOverride ov;
+    ov.h2d = host_lines;
+    ov.h2d_pieces = pieces;
+    int rc;
+    {
+        DeviceGuard g(e->device);
+        rc = xs::engine_execute(e, opt, conds, ncond, dev_lines, grid, out, out_stride, &ov);
+        if (rc == XS_OK && host_out && ncond > 0 && grid->points > 0) {
+            // the chunk's span of every condition's row, rows out_stride apart
+            const size_t pitch = sizeof(double) * (ncond > 1 ? out_stride : size_t(grid->start_idx + grid->points));
+            const size_t at = size_t(grid->start_idx);
+            XS_CU(cudaMemcpy2DAsync(host_out + at, pitch, out + at, pitch, sizeof(double) * size_t(grid->points),
+                                    size_t(ncond), cudaMemcpyDeviceToHost, e->stream));
+        }
+    }
+    return rc;
 }
 
 double xs_error_bound(int profile, int precision) {
@@ -376,6 +417,12 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     const bool streamed = ov && ov->s32;
     if (streamed && (kind != XS_VOIGT || opt->convention != XS_CONV_GPU || !ov->gl32))
         return fail(XS_ERR_UNSUPPORTED, "precomputed intensities: VOIGT, GPU convention, with gamma");
+    const int h2d_pieces = (ov && ov->h2d) ? std::max(1, std::min(ov->h2d_pieces, kMaxPieces)) : 0;
+    if (h2d_pieces && (streamed || (ov->tc_s != nullptr)))
+        return fail(XS_ERR_INVALID, "host lines: not with precomputed intensities or caches");
+    const int tc_mode = (ov && ov->tc_s) ? ov->tc_mode : 0;
+    if (tc_mode && (streamed || ncond != 1 || tc_mode < 1 || tc_mode > 2 || (kind == XS_VOIGT && !ov->tc_pw)))
+        return fail(XS_ERR_INVALID, "per-temperature cache: one condition, S (and Voigt's power) arrays");
     if (lines->count > 0 && (!lines->nu || (!streamed && (!lines->energies || !lines->aif || !lines->gns))))
         return fail(XS_ERR_INVALID, "line arrays missing");
     if (kind == XS_VOIGT && lines->count > 0 && !streamed && (!lines->gamma || !lines->n))
@@ -573,8 +620,15 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
     L.n = n;
     L.s32 = streamed ? ov->s32 : nullptr;
     L.gl32 = streamed ? ov->gl32 : nullptr;
+    L.tc_s = tc_mode ? ov->tc_s : nullptr;
+    L.tc_pw = tc_mode ? ov->tc_pw : nullptr;
+    L.tc_mode = tc_mode;
 
     const cudaStream_t st = e->stream;
+    if (h2d_pieces && !e->copy_stream) {
+        XS_CU(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
+        for (auto& ev : e->pev) XS_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
     const bool timing = !(ov && ov->no_timing);
     // Inside a stream capture the timing events must become event-record
     // nodes of the graph (cudaEventRecordExternal); outside one, a plain
@@ -646,9 +700,47 @@ int engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* cond
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[0], st, ev_flags);
         err = cudaMemsetAsync(pa.kc, 0, sizeof(int) * size_t(kKcWords), st);
         if (err != cudaSuccess) return cuda_fail(err, "core-width reset");
-        err = launch_prep(kind, opt->convention, mixed, pa, st);
-        if (err != cudaSuccess) return cuda_fail(err, "step one launch");
-        ++launched;
+        if (c0 == 0 && h2d_pieces > 0) {
+            // host lines: slice k is copied on the copy stream (after the
+            // work already on this stream, which may still read the device
+            // lines) and step one starts on it when its copy is done
+            err = cudaEventRecord(e->pev[kMaxPieces], st);
+            if (err == cudaSuccess) err = cudaStreamWaitEvent(e->copy_stream, e->pev[kMaxPieces], 0);
+            const size_t total = lines->count;
+            for (int k = 0; k < h2d_pieces && err == cudaSuccess; ++k) {
+                const size_t a0 = total * size_t(k) / size_t(h2d_pieces);
+                const size_t a1 = total * size_t(k + 1) / size_t(h2d_pieces);
+                if (a1 <= a0) continue;
+                auto cp = [&](const void* dst, const void* src, size_t elem) {
+                    if (err == cudaSuccess && src && dst)
+                        err = cudaMemcpyAsync(static_cast<char*>(const_cast<void*>(dst)) + a0 * elem,
+                                              static_cast<const char*>(src) + a0 * elem, (a1 - a0) * elem,
+                                              cudaMemcpyHostToDevice, e->copy_stream);
+                };
+                const xs_lines* hl = ov->h2d;
+                cp(lines->nu, hl->nu, sizeof(double));
+                cp(lines->energies, hl->energies, sizeof(double));
+                cp(lines->aif, hl->aif, sizeof(double));
+                cp(lines->gns, hl->gns, sizeof(int));
+                cp(lines->gamma, hl->gamma, sizeof(double));
+                cp(lines->n, hl->n, sizeof(double));
+                if (err == cudaSuccess) err = cudaEventRecord(e->pev[k], e->copy_stream);
+                if (err == cudaSuccess) err = cudaStreamWaitEvent(st, e->pev[k], 0);
+                // the lines step one evaluates stop at n (CPU coverage rule)
+                pa.line0 = long(std::min(a0, size_t(n)));
+                pa.line1 = long(std::min(a1, size_t(n)));
+                if (err == cudaSuccess && pa.line1 > pa.line0) {
+                    err = launch_prep(kind, opt->convention, mixed, pa, st);
+                    ++launched;
+                }
+            }
+            pa.line0 = pa.line1 = 0;
+            if (err != cudaSuccess) return cuda_fail(err, "host lines: copy or step one");
+        } else {
+            err = launch_prep(kind, opt->convention, mixed, pa, st);
+            if (err != cudaSuccess) return cuda_fail(err, "step one launch");
+            ++launched;
+        }
         if (timing && c0 == 0) cudaEventRecordWithFlags(e->ev[1], st, ev_flags);
 
         StepArgs sa;

@@ -22,6 +22,14 @@ struct ExecOverride {
     double beta = 0.0;            //   the cross_section_data the caller copied)
     const float* s32 = nullptr;   // streamed Voigt lines: S(T) and gamma(T, P)
     const float* gl32 = nullptr;  //   per line (see LinesDev)
+    // Line list in host memory, copied to the call's (device) lines in
+    // h2d_pieces slices on the engine's copy stream; step one starts on each
+    // slice as its copy completes.
+    const xs_lines* h2d = nullptr;
+    int h2d_pieces = 0;
+    double* tc_s = nullptr;       // per-temperature cache of S(T) and
+    double* tc_pw = nullptr;      //   (T_ref/T)^n (one condition; see
+    int tc_mode = 0;              //   LinesDev)
     mutable int kernels = 0;      // out: kernels the call launched (added to)
 };
 

@@ -191,10 +191,21 @@ struct LinesDev {
     // when set, energies, aif, gns, gamma and nexp are not read.
     const float* s32;
     const float* gl32;
+    // Per-temperature cache (one condition, single-condition layouts): the
+    // intensity S(T) and, for Voigt, the Lorentz temperature power
+    // (T_ref/T)^n of each line as step one computes them, FP64.  tc_mode 1:
+    // step one reads them instead of computing them (and reads no E'', A, g
+    // or n); 2: it computes and stores them.
+    double* tc_s;
+    double* tc_pw;
+    int tc_mode;
 };
 
 struct PrepArgs {
     LinesDev L;
+    // Lines [line0, line1) of the list (line1 = 0: to L.n): step one can run
+    // on a list in slices, each as soon as its copy to the device is done.
+    long line0, line1;
     GridDev G;
     int ncond;
     CondDev cond[kMaxCond];

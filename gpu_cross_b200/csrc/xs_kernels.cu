@@ -208,9 +208,12 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
     const double nu = a.L.nu[i];
     if (c == 0 && i > 0 && nu < a.L.nu[i - 1]) atomicOr(a.err, kErrUnsorted);
     const bool streamed = KIND == kVoigt && CONV == kConvGpu && a.L.s32 != nullptr;
-    const double ei = streamed ? 0.0 : a.L.energies[i];
-    const double aif = streamed ? 0.0 : a.L.aif[i];
-    const double gns = streamed ? 0.0 : double(a.L.gns[i]);
+    // per-temperature cache: read S(T) and (T_ref/T)^n, or compute and store
+    const bool tc_read = a.L.tc_mode == 1, tc_write = a.L.tc_mode == 2;
+    const bool from_lines = !streamed && !tc_read;
+    const double ei = from_lines ? a.L.energies[i] : 0.0;
+    const double aif = from_lines ? a.L.aif[i] : 0.0;
+    const double gns = from_lines ? double(a.L.gns[i]) : 0.0;
     const double cut = C.cut;
     const size_t ci = size_t(c) * size_t(a.L.n) + size_t(i);
     int kcl = 0;
@@ -225,11 +228,15 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
             if (nu_if == 0) nu_if = 1e-6;
             if (streamed) {
                 S = double(a.L.s32[i]);
+            } else if (tc_read) {
+                S = a.L.tc_s[i];
             } else {
                 S = C.cmcoef * aif * gns * kISQRTPI * exp(-C.beta * ei) * (1.0 - exp(-C.beta * nu_if)) /
                     (nu_if * nu_if * C.partition);
                 if (gns == -1) S = aif;
             }
+        } else if (tc_read) {
+            S = a.L.tc_s[i];
         } else {
             // doppler_stepone / stepone, cross_kernal.cu:645-648, :487-490
             S = C.cmcoef * aif * gns * exp(-C.beta * ei) * (1.0 - exp(-C.beta * nu)) /
@@ -254,7 +261,9 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
         // OpenMPManager::ComputeVoigt / ComputeDoppler, OpenMPManager.cpp:196-208, :151-163
         double nu_if = nu;
         if (nu_if == 0) nu_if = 1e-6;
-        if (KIND == kVoigt)
+        if (tc_read)
+            S = a.L.tc_s[i];
+        else if (KIND == kVoigt)
             S = C.cmcoef * aif * gns * kISQRTPI * exp(-C.beta * ei) * (1.0 - exp(-C.beta * nu_if)) /
                 (nu_if * nu_if * C.partition);
         else
@@ -271,9 +280,14 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
         // keep their window (monotone arrays) and add exactly 0 below.
     }
 
+    if (tc_write) a.L.tc_s[i] = S;
     if (KIND == kVoigt) {
-        const double gl = streamed ? double(a.L.gl32[i])
-                                   : a.L.gamma[i] * C.gamma_scale * pow(C.tratio, a.L.nexp[i]);
+        double pw = 0.0;
+        if (!streamed) {
+            pw = tc_read ? a.L.tc_pw[i] : pow(C.tratio, a.L.nexp[i]);
+            if (tc_write) a.L.tc_pw[i] = pw;
+        }
+        const double gl = streamed ? double(a.L.gl32[i]) : a.L.gamma[i] * C.gamma_scale * pw;
         const double g = 1.0 / (nu_p * C.dpw);  // gammaG, cross_kernal.cu:958
         const double y = gl * g;
         const double pref = (CONV == kConvCpu && S == 0.0) ? 0.0 : S * g;
@@ -431,10 +445,10 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
 
 template <int KIND, int CONV, bool MIXED>
 __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long i = a.line0 + long(blockIdx.x) * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
     int kcl = 0, rch = 0;
-    if (i < a.L.n) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, &rch);
+    if (i < (a.line1 > 0 ? a.line1 : a.L.n)) kcl = prep_line<KIND, CONV, MIXED>(a, i, c, &rch);
     if (KIND == kVoigt) {
         // Block maxima of the core widths (kc) and, mixed, of the core pass's
         // reach (kc + kMaxCond), one atomic each per block.
@@ -476,9 +490,9 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
     extern __shared__ __align__(16) double cls[];  // [3][ncache][256]: S, (T_ref/T)^n, g
     __shared__ int smax[2][kMaxCond][8];
     const int ngroups = a.ncond / C;
-    const long i = long(blockIdx.x) * 256 + threadIdx.x;
+    const long i = a.line0 + long(blockIdx.x) * 256 + threadIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool live = i < a.L.n;
+    const bool live = i < (a.line1 > 0 ? a.line1 : a.L.n);
     const double* F = a.G.freq;
     const double f0 = F[0];
     const double df = a.G.df;
@@ -2401,12 +2415,13 @@ cudaError_t launch_reduce_splits(const StepArgs& a, int ncond_out, cudaStream_t 
 }
 
 cudaError_t launch_prep(int kind, int conv, bool mixed, const PrepArgs& a, cudaStream_t stream) {
-    if (a.L.n <= 0 || a.ncond <= 0) return cudaSuccess;
-    const dim3 grid(unsigned((a.L.n + 255) / 256), unsigned(a.ncond));
+    const long count = (a.line1 > 0 ? a.line1 : a.L.n) - a.line0;
+    if (count <= 0 || a.ncond <= 0) return cudaSuccess;
+    const dim3 grid(unsigned((count + 255) / 256), unsigned(a.ncond));
     if (kind == kVoigt && mixed && a.group > 0) {
         // (precomputed-intensity lists run one condition at a time)
         if (a.L.s32 != nullptr || a.ncond % a.group != 0) return cudaErrorInvalidValue;
-        const unsigned nblk = unsigned((a.L.n + 255) / 256);
+        const unsigned nblk = unsigned((count + 255) / 256);
         const int ncache = a.nclass <= kMaxClassCache ? a.nclass : 0;
         const size_t smem = sizeof(double) * 3 * size_t(ncache) * 256;
         auto go = [&](auto kernel) {

@@ -33,6 +33,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "xs_engine.h"
@@ -259,6 +260,37 @@ struct Molecule {
     }
 };
 
+// Per-temperature intensity cache of one molecule, profile, T and Q(T):
+// S(T) and, for Voigt, (T_ref/T)^n of every line, as step one computes them.
+// `covered`: line ranges stored by completed chunks (sorted, disjoint).
+struct TCache {
+    int mol = -1, profile = 0;
+    double T = 0.0, Q = 0.0;
+    double* s = nullptr;
+    double* pw = nullptr;
+    size_t bytes = 0;
+    std::vector<std::pair<size_t, size_t>> covered;
+    int refs = 0;                 // admitted requests that use it
+    unsigned long long used = 0;  // last use (least recently used goes first)
+    bool covers(size_t l0, size_t l1) const {
+        for (const auto& c : covered)
+            if (c.first <= l0 && l1 <= c.second) return true;
+        return false;
+    }
+    void add(size_t l0, size_t l1) {
+        covered.emplace_back(l0, l1);
+        std::sort(covered.begin(), covered.end());
+        std::vector<std::pair<size_t, size_t>> m;
+        for (const auto& c : covered) {
+            if (!m.empty() && c.first <= m.back().second)
+                m.back().second = std::max(m.back().second, c.second);
+            else
+                m.push_back(c);
+        }
+        covered.swap(m);
+    }
+};
+
 struct Request {
     unsigned long long id = 0;
     xs_request q{};
@@ -274,6 +306,8 @@ struct Request {
     size_t dev_bytes = 0, host_off = SIZE_MAX, host_bytes = 0;
     Clock::time_point t_submit, t_admit, t_done;
     unsigned long long last_issue = 0;  // round robin: issue order of its last chunk
+    int tc = -1;                        // per-temperature cache in use (index)
+    int tc_chunks = 0;                  // chunks that read it
     int status = XS_OK;
     std::string error;
     bool done = false;
@@ -283,6 +317,8 @@ struct Flight {
     Request* r;
     cudaEvent_t ev;
     bool last;
+    int tc_wrote;        // cache the chunk stored into (-1: none) ...
+    size_t l0, l1;       // ... for these lines
 };
 
 struct Lane {
@@ -302,6 +338,12 @@ struct xs_server {
     std::vector<Molecule> mols;
     std::vector<Lane> lanes;
     unsigned long long issue_seq = 0;  // chunks issued (round robin order)
+    // per-temperature caches (scheduler-owned); keys seen once are remembered
+    // so that a cache is made on a key's second request
+    std::vector<TCache> tcache;
+    size_t tc_used = 0;
+    unsigned long long tc_clock = 0;
+    std::deque<std::tuple<int, int, double, double>> tc_seen;
     Arena arena;
     std::vector<cudaEvent_t> ev_pool;
 
@@ -357,8 +399,87 @@ cudaEvent_t take_event(xs_server* s) {
     return e;
 }
 
+// Frees a per-temperature cache that no request holds (cudaFree waits for
+// the device; caches are made and dropped rarely: on a key's second request,
+// and when room is needed).
+void tc_drop(xs_server* s, size_t k) {
+    TCache& e = s->tcache[k];
+    cudaFree(e.s);
+    s->tc_used -= e.bytes;
+    e = TCache{};
+}
+
+// Drops the least recently used cache that no request holds; false when
+// there is none.
+bool tc_drop_lru(xs_server* s) {
+    int victim = -1;
+    for (size_t k = 0; k < s->tcache.size(); ++k) {
+        const TCache& e = s->tcache[k];
+        if (e.s && e.refs == 0 && (victim < 0 || e.used < s->tcache[size_t(victim)].used)) victim = int(k);
+    }
+    if (victim < 0) return false;
+    tc_drop(s, size_t(victim));
+    return true;
+}
+
+// The per-temperature cache of an admitted request's key (molecule, profile,
+// T, Q): an existing one, or a new one on the key's second request when it
+// fits the budgets; -1: none.
+int tc_acquire(xs_server* s, Request* r) {
+    if (s->cfg.tcache_bytes < 0) return -1;
+    const int mol = r->q.molecule, prof = r->q.profile;
+    const double T = r->q.temperature, Q = r->cond.partition;
+    for (size_t k = 0; k < s->tcache.size(); ++k) {
+        TCache& e = s->tcache[k];
+        if (e.s && e.mol == mol && e.profile == prof && e.T == T && e.Q == Q) {
+            ++e.refs;
+            e.used = ++s->tc_clock;
+            return int(k);
+        }
+    }
+    const auto key = std::make_tuple(mol, prof, T, Q);
+    auto it = std::find(s->tc_seen.begin(), s->tc_seen.end(), key);
+    if (it == s->tc_seen.end()) {
+        s->tc_seen.push_back(key);
+        if (s->tc_seen.size() > 256) s->tc_seen.pop_front();
+        return -1;
+    }
+    s->tc_seen.erase(it);
+    const size_t n = s->mols[size_t(mol)].n;
+    const size_t bytes = sizeof(double) * n * (prof == XS_VOIGT ? 2 : 1);
+    const size_t cap = size_t(s->cfg.tcache_bytes);
+    auto fits = [&]() {
+        return s->tc_used + bytes <= cap &&
+               s->resident + s->dev_requests + s->tc_used + bytes <= s->cfg.device_budget;
+    };
+    while (!fits())
+        if (!tc_drop_lru(s)) return -1;
+    double* d = nullptr;
+    if (cudaMalloc(reinterpret_cast<void**>(&d), bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    size_t k = 0;
+    while (k < s->tcache.size() && s->tcache[k].s) ++k;
+    if (k == s->tcache.size()) s->tcache.emplace_back();
+    TCache& e = s->tcache[k];
+    e.mol = mol;
+    e.profile = prof;
+    e.T = T;
+    e.Q = Q;
+    e.s = d;
+    e.pw = prof == XS_VOIGT ? d + n : nullptr;
+    e.bytes = bytes;
+    e.refs = 1;
+    e.used = ++s->tc_clock;
+    s->tc_used += bytes;
+    return int(k);
+}
+
 void finish(xs_server* s, Request* r) {
     Lane& ln = s->lanes[size_t(r->lane)];
+    if (r->tc >= 0) --s->tcache[size_t(r->tc)].refs;
+    r->tc = -1;
     if (r->d_freq) cudaFreeAsync(r->d_freq, ln.st);
     if (r->d_out) cudaFreeAsync(r->d_out, ln.st);
     r->d_freq = r->d_out = nullptr;
@@ -408,7 +529,9 @@ enum class Admit { kAdmitted, kNoRoom, kFailed };
 
 Admit admit(xs_server* s, Request* r) {
     const size_t host = sizeof(double) * size_t(r->q.npoints);
-    if (s->resident + s->dev_requests + r->dev_bytes > s->cfg.device_budget) return Admit::kNoRoom;
+    // requests come before caches: drop caches no request holds for room
+    while (s->resident + s->dev_requests + s->tc_used + r->dev_bytes > s->cfg.device_budget)
+        if (!tc_drop_lru(s)) return Admit::kNoRoom;
     size_t off;
     {
         std::lock_guard<std::mutex> lk(s->mu);  // the arena is shared with xs_server_wait
@@ -448,6 +571,7 @@ Admit admit(xs_server* s, Request* r) {
     }
     s->dev_requests += r->dev_bytes;
     ln.load += r->remaining;
+    r->tc = tc_acquire(s, r);
     r->t_admit = Clock::now();
     s->active.push_back(r);
     s->n_active = int(s->active.size());
@@ -460,6 +584,7 @@ bool issue(xs_server* s, Request* r) {
     Lane& ln = s->lanes[size_t(r->lane)];
     const Molecule& m = s->mols[size_t(r->q.molecule)];
     const ChunkPlan& c = r->chunks[r->next++];
+    int wrote = -1;
     if (r->status == XS_OK) {
         xs_lines L;
         L.nu = m.nu + c.l0;
@@ -472,8 +597,23 @@ bool issue(xs_server* s, Request* r) {
         xs_grid G{r->d_freq, r->q.npoints, c.start, c.points};
         xs::ExecOverride ov;
         ov.no_timing = true;
+        if (r->tc >= 0) {
+            // step one reads the cached S(T) of lines that completed chunks
+            // stored, else computes and stores them
+            const TCache& e = s->tcache[size_t(r->tc)];
+            ov.tc_s = e.s + c.l0;
+            ov.tc_pw = e.pw ? e.pw + c.l0 : nullptr;
+            if (e.covers(c.l0, c.l1)) {
+                ov.tc_mode = 1;
+                ++r->tc_chunks;
+            } else {
+                ov.tc_mode = 2;
+                wrote = r->tc;
+            }
+        }
         const int rc = xs::engine_execute(ln.eng, &r->opt, &r->cond, 1, &L, &G, r->d_out, 0, &ov);
         if (rc != XS_OK) {
+            wrote = -1;  // nothing was stored
             r->status = rc;
             r->error = xs_last_error();
             if (rc == XS_ERR_CUDA) return false;
@@ -490,7 +630,7 @@ bool issue(xs_server* s, Request* r) {
     }
     cudaEvent_t ev = take_event(s);
     if (!ev || cudaEventRecord(ev, ln.st) != cudaSuccess) return false;
-    ln.flight.push_back({r, ev, last});
+    ln.flight.push_back({r, ev, last, wrote, c.l0, c.l1});
     return true;
 }
 
@@ -536,6 +676,7 @@ void scheduler(xs_server* s) {
                 }
                 ln.flight.pop_front();
                 s->ev_pool.push_back(f.ev);
+                if (f.tc_wrote >= 0) s->tcache[size_t(f.tc_wrote)].add(f.l0, f.l1);
                 if (f.last) finish(s, f.r);
                 progress = true;
             }
@@ -627,6 +768,7 @@ int xs_server_create(int device, const xs_server_config* cfg, xs_server** out) {
     if (c.lanes > 16 || c.depth > 8) return sfail(XS_ERR_INVALID, "xs_server_create: lanes <= 16, depth <= 8");
     if (c.policy != XS_POLICY_LEAST_WORK && c.policy != XS_POLICY_ROUND_ROBIN)
         return sfail(XS_ERR_INVALID, "xs_server_create: unknown policy");
+    if (c.tcache_bytes == 0) c.tcache_bytes = 4LL << 30;
     auto* s = new xs_server();
     s->device = device;
     s->cfg = c;
@@ -722,6 +864,7 @@ int xs_server_destroy(xs_server* s) {
         cudaStreamDestroy(l.st);
     }
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    for (TCache& e : s->tcache) cudaFree(e.s);
     if (s->aux) cudaStreamDestroy(s->aux);
     cudaFree(s->d_pwork);
     for (Molecule& m : s->mols) {
@@ -932,6 +1075,7 @@ int xs_server_wait(xs_server* s, unsigned long long id, double* out, int npoints
         info->line_evals = r->pairs;
         info->lines = r->lines;
         info->err_bound = xs_error_bound(r->opt.profile, r->opt.precision);
+        info->tcache_chunks = r->tc_chunks;
     }
     int rc = r->status;
     std::string err = r->error;

@@ -196,6 +196,22 @@ size_t xs_scratch_bytes_needed(const xs_options* opt, int ncond, size_t n_lines)
 int xs_engine_execute(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
                       const xs_lines* lines, const xs_grid* grid, double* out, size_t out_stride);
 
+/* xs_engine_execute with the line list in host memory (pinned, for the
+ * copies to overlap): host_lines is copied into dev_lines (the same count;
+ * device arrays the call then evaluates, as in xs_engine_execute) in
+ * `pieces` (1..16) slices on the engine's copy stream, and step one starts
+ * on each slice as soon as its copy is done, so the copies overlap step one.
+ * When host_out is not NULL, each condition's span [start_idx, start_idx +
+ * points) of out is copied to the same place of host_out (rows out_stride
+ * apart) after the call's work.  Asynchronous on the engine's stream:
+ * xs_engine_sync before reading host_out or reusing the host arrays.  This is
+ * the host-buffer form of the reference's GpuManager::TransferVectors ->
+ * ExecuteCrossSection -> TransferResults sequence (GPUManager.cpp:87-106,
+ * :107-121, :160-168). */
+int xs_engine_execute_host(xs_engine* e, const xs_options* opt, const xs_condition* conds, int ncond,
+                           const xs_lines* host_lines, const xs_lines* dev_lines, const xs_grid* grid,
+                           double* out, size_t out_stride, double* host_out, int pieces);
+
 /* Error statement of the last execute (or graph replay), against the FP64
  * arithmetic of the same reference convention (no counterpart in the
  * reference, which computes in FP64 only).
@@ -375,6 +391,16 @@ typedef struct {
                              XS_POLICY_LEAST_WORK (0, default): the one with
                              the least remaining work; XS_POLICY_ROUND_ROBIN:
                              each in turn (processor sharing by chunks) */
+    long long tcache_bytes; /* device bytes (within device_budget) for the
+                             per-temperature intensity caches (0 = 4 GiB;
+                             < 0: none).  A cache holds, for one molecule,
+                             profile, T and Q(T), every line's S(T) and, for
+                             Voigt, (T_ref/T)^n in FP64, exactly as step one
+                             computes them; it is made on the second request
+                             with that key, filled by the chunks that run, and
+                             read by later chunks over the same lines instead
+                             of recomputing (least recently used caches that
+                             no request holds are dropped for room). */
 } xs_server_config;
 #define XS_POLICY_LEAST_WORK 0
 #define XS_POLICY_ROUND_ROBIN 1
@@ -407,6 +433,8 @@ typedef struct {
                            point and of the band integral against the FP64
                            arithmetic (xs_error_bound of the request's profile
                            and precision) */
+    int tcache_chunks;  /* chunks whose step one read the per-temperature
+                           cache instead of computing S(T) */
 } xs_request_info;
 
 int xs_server_create(int device, const xs_server_config* cfg, xs_server** out);

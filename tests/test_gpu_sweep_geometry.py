@@ -129,3 +129,39 @@ def test_single_point_reduced_vs_reference_kernel(cuda):
     assert chunks > 1
     assert_fp64_parity(outs[capi.FP64], ref)
     assert_mixed_parity(outs[capi.MIXED], outs[capi.FP64])
+
+
+@pytest.mark.parametrize("precision, C, pieces", [(capi.MIXED, 8, 8), (capi.FP64, 2, 5), (capi.MIXED, 1, 3)])
+def test_execute_host_matches_execute(cuda, sweep, precision, C, pieces):
+    """xs_engine_execute_host (pinned host lines copied in slices that overlap
+    step one, result copied back) gives the bit-identical result of
+    xs_engine_execute on the same lines already on the device."""
+    import torch
+
+    lines, grid, conds, common, fr, d, dfr, cc = sweep
+    if C == 1:
+        cc = cc[:1]
+    nc = len(cc)
+    opts = capi.make_options(capi.VOIGT, grid.dfreq, common["mean_mass"], precision=precision,
+                             ref_temp=common["ref_temp"], warps_per_block=4, conditions_per_warp=C)
+    stream = torch.cuda.current_stream(cuda)
+    eng = capi.Engine(cuda.index)
+    try:
+        eng.set_stream(stream.cuda_stream)
+        want = torch.zeros((nc, len(fr)), dtype=torch.float64, device=cuda)
+        eng.execute(opts, cc, capi.make_lines(d), capi.make_grid(dfr), want.data_ptr(), len(fr))
+        eng.sync()
+        host = {k: torch.from_numpy(np.ascontiguousarray(getattr(lines, k))).pin_memory()
+                for k in ("nu", "energies", "aif", "gns", "gamma", "n")}
+        dev = {k: torch.empty_like(v, device=cuda) for k, v in host.items()}  # filled by the call
+        out = torch.zeros_like(want)
+        out_host = torch.full((nc, len(fr)), -1.0, dtype=torch.float64).pin_memory()
+        eng.execute_host(opts, cc, capi.make_lines(host), capi.make_lines(dev), capi.make_grid(dfr),
+                         out.data_ptr(), len(fr), out_host.data_ptr(), pieces=pieces)
+        eng.sync()
+    finally:
+        eng.close()
+    for k in host:
+        assert torch.equal(dev[k].cpu(), host[k])
+    np.testing.assert_array_equal(out.cpu().numpy(), want.cpu().numpy())
+    np.testing.assert_array_equal(out_host.numpy(), want.cpu().numpy())

@@ -129,6 +129,39 @@ def test_same_result_alone_and_in_a_mix(cuda, molecule, policy):
             assert_mixed_parity(alone[i], want)
 
 
+@pytest.mark.parametrize("prof, prec", [(capi.VOIGT, capi.FP64), (capi.VOIGT, capi.MIXED),
+                                        (capi.DOPPLER, capi.FP64)])
+def test_per_temperature_cache(cuda, molecule, prof, prec):
+    """Requests with one (molecule, profile, T, Q) key: the second makes the
+    cache and fills it, the third reads it on every chunk, and all three
+    results are bit-identical to a server without caches."""
+    n = 30000
+    base = dict(profile=prof, precision=prec, temperature=1234.0, partition=2345.5, f0=1000.0, df=0.01,
+                npoints=n, cut=25.0)
+    pressures = (0.3, 1.7, 0.3)
+
+    def run(tcache_bytes):
+        srv = capi.Server(0, lanes=2, chunk_pairs=2e7 if prof == capi.VOIGT else 2e4,
+                          tcache_bytes=tcache_bytes)
+        try:
+            mid = srv.add_molecule(molecule, MASS)
+            return [srv.wait(srv.submit(molecule=mid, pressure=P, **base), n) for P in pressures]
+        finally:
+            srv.close()
+
+    cached, plain = run(0), run(-1)
+    infos = [info for _, info in cached]
+    assert all(info["status"] == 0 for info in infos) and infos[0]["chunks"] > 3
+    assert infos[0]["tcache_chunks"] == 0 and infos[1]["tcache_chunks"] == 0
+    assert infos[2]["tcache_chunks"] == infos[2]["chunks"]
+    assert all(info["tcache_chunks"] == 0 for _, info in plain)
+    for (got, _), (want, _) in zip(cached, plain):
+        np.testing.assert_array_equal(got, want)
+    # a different pressure changes a Voigt result: the cache key does not hold it
+    if prof == capi.VOIGT:
+        assert not np.array_equal(cached[0][0], cached[1][0])
+
+
 def server_resident_bytes(lanes, chunk_lines):
     """What xs_server_create reserves: per lane the largest Voigt scratch
     for chunk_lines lines, 64 MiB for line-split parts, plus 4 MiB."""
