@@ -659,6 +659,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -1505,7 +1509,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt_mc(StepArgs a) {
 // two occupancy points the autotuner chooses between through the block size.
 template <int C, int WARPS>
 constexpr int voigt_mcx_min_blocks() {
-    return (C == 8 && WARPS == 8) ? 2 : 24 / WARPS;
+    return (C == 8 && WARPS == 8) ? 2 : (C == 8 && WARPS == 4) ? 7 : 24 / WARPS;
 }
 
 template <int C, int WARPS>
@@ -1517,8 +1521,12 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     using R1 = LineR1<C>;
-    LineShX* lsb = reinterpret_cast<LineShX*>(smem_raw) + warp * 64;
-    R1* rb = reinterpret_cast<R1*>(smem_raw + size_t(WARPS) * 64 * sizeof(LineShX)) + warp * 64;
+    // staged per line: the offsets and flags of LineShX (16 B), its window
+    // (8 B) and the group's region-I records; a whole line's FP64 centre is
+    // read from memory when needed
+    float4* lsb = reinterpret_cast<float4*>(smem_raw) + warp * 64;
+    int2* lhb = reinterpret_cast<int2*>(smem_raw + size_t(WARPS) * 64 * sizeof(float4)) + warp * 64;
+    R1* rb = reinterpret_cast<R1*>(smem_raw + size_t(WARPS) * 64 * (sizeof(float4) + sizeof(int2))) + warp * 64;
 
     for (;;) {
         int item = 0;
@@ -1660,7 +1668,10 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
         const int ngroups = split_groups(Lb - La, a.splits, split);
         auto gstart = [&](int gi) { return La + 32 * (split + gi * a.splits); };
         auto stage_group = [&](int bufi, int b, int cnt) {
-            stage(lsb + bufi * 32, lsh + b, cnt, lane);
+            if (lane < cnt) {
+                cp_async16(lsb + bufi * 32 + lane, lsh + b + lane);
+                cp_async8(lhb + bufi * 32 + lane, &lsh[b + lane].lo);
+            }
             stage(rb + bufi * 32, r1 + b, cnt, lane);
         };
         if (ngroups > 0) {
@@ -1679,7 +1690,8 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                 cp_async_wait<0>();
             }
             __syncwarp();
-            const LineShX* SL = lsb + (gi & 1) * 32;
+            const float4* SL = lsb + (gi & 1) * 32;  // m, df/nu, r/nu, flags
+            const int2* SW = lhb + (gi & 1) * 32;    // window [lo, hi)
             const R1* SR = rb + (gi & 1) * 32;
             const int gb = gstart(gi);
             const int ge = Lb - gb < 32 ? Lb : gb + 32;
@@ -1754,12 +1766,12 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             auto pair_run = [&](int x, int y, auto full) {
                 auto in_of = [&](int t) {
                     if constexpr (decltype(full)::value) return true;
-                    else return jj >= SL[t].lo && jj < SL[t].hi && jj < t1;
+                    else return jj >= SW[t].x && jj < SW[t].y && jj < t1;
                 };
                 int t = x;
                 for (; t + 1 < y; t += 2) {
-                    const float4 sA = *reinterpret_cast<const float4*>(&SL[t]);
-                    const float4 sB = *reinterpret_cast<const float4*>(&SL[t + 1]);
+                    const float4 sA = SL[t];
+                    const float4 sB = SL[t + 1];
                     const float XA = fmaf(sA.x - jf, sA.y, sA.z);
                     const float XB = fmaf(sB.x - jf, sB.y, sB.z);
                     const int fA = __float_as_int(sA.w), fB = __float_as_int(sB.w);
@@ -1772,7 +1784,7 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     }
                 }
                 if (t < y) {
-                    const float4 s = *reinterpret_cast<const float4*>(&SL[t]);
+                    const float4 s = SL[t];
                     const float X = fmaf(s.x - jf, s.y, s.z);
                     line_region1(X * X, SR[t], (__float_as_int(s.w) & kLineWide) != 0, in_of(t));
                 }
@@ -1788,13 +1800,14 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
             // u).
             auto cand_run = [&](int x, int y) {
                 for (int t = x; t < y; ++t) {
-                    const LineShX s = SL[t];
+                    const float4 s = SL[t];
+                    const int flags = __float_as_int(s.w);
                     const bool full = (t >= a1 && t < d1);
-                    const bool in = full || (jj >= s.lo && jj < s.hi && jj < t1);
+                    const bool in = full || (jj >= SW[t].x && jj < SW[t].y && jj < t1);
                     if constexpr (NP % 2 == 0) {
-                        if (!(s.flags & (kLineWhole | kLineWide))) {
+                        if (!(flags & (kLineWhole | kLineWide))) {
                             // narrow: the shared reciprocal
-                            const float X = fmaf(s.m - jf, s.dfn, s.rn);
+                            const float X = fmaf(s.x - jf, s.y, s.z);
 #pragma unroll
                             for (int p = 0; p < NP; p += 2) region1_ab_near(X * X, SR[t], p, p + 1, in);
                             continue;
@@ -1802,8 +1815,10 @@ __global__ void __launch_bounds__(WARPS * 32, (voigt_mcx_min_blocks<C, WARPS>())
                     }
                     // whole lines: X from the FP64 centre (rare; the grid
                     // value is read here rather than held for every line)
-                    const float X = (s.flags & kLineWhole) ? float((s.nu - a.G.freq[jj < t1 ? jj : tl]) / s.nu)
-                                            : fmaf(s.m - jf, s.dfn, s.rn);
+                    double nu = 0.0;
+                    if (flags & kLineWhole) nu = lsh[gb + t].nu;
+                    const float X = (flags & kLineWhole) ? float((nu - a.G.freq[jj < t1 ? jj : tl]) / nu)
+                                                         : fmaf(s.x - jf, s.y, s.z);
                     const float X2 = X * X;
                     const float aX = fabsf(X);
 #pragma unroll
@@ -2286,7 +2301,7 @@ cudaError_t run_voigt_mc(int blocks, const StepArgs& a, cudaStream_t st, int* oc
 
 template <int C, int WARPS>
 cudaError_t run_voigt_mcx(int blocks, const StepArgs& a, cudaStream_t st, int* occ) {
-    const size_t smem = size_t(WARPS) * 64 * (sizeof(LineShX) + sizeof(LineR1<C>));
+    const size_t smem = size_t(WARPS) * 64 * (sizeof(float4) + sizeof(int2) + sizeof(LineR1<C>));
     if (smem > 48 * 1024) {
         if (cudaFuncSetAttribute(k_steptwo_voigt_mcx<C, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)) != cudaSuccess)
