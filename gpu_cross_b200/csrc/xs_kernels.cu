@@ -183,9 +183,29 @@ __device__ __forceinline__ void region_interval_q(double nu, double g, double y,
     jlo = 1;
     jhi = 0;
     if (!(y < lim) || lo >= hi) return;
+    const double hq = (lim - y) * q;
+    // x_j = (md - j) / q, so the points inside are the integers of
+    // (md - hq, md + hq).  The region test's roundings (f_j, nu - f_j, the
+    // product with g, md and hq themselves) move both ends by a few 1e-16 of
+    // |md|, (|nu| + |f0|) / df and hq grid steps; where each end lies further
+    // than `tol` (a thousand times that, and at least 1e-6) from an integer,
+    // the exact region test of every point agrees with [ceil(md - hq),
+    // ceil(md + hq) - 1], clamped to the window, and is not evaluated.
+    // Otherwise the walks below decide.
+    {
+        const double bl = md - hq, bh = md + hq;
+        const double tol = 1.0e-6 + 1.0e-13 * (fabs(md) + (fabs(nu) + fabs(f0)) / df + hq);
+        if (fabs(bl) < 1.0e9 && fabs(bh) < 1.0e9 && fabs(bl - rint(bl)) > tol && fabs(bh - rint(bh)) > tol) {
+            const int jl = clamp_index(ceil(bl), lo, hi), jh = clamp_index(ceil(bh), lo, hi);
+            if (jl < jh) {
+                jlo = jl;
+                jhi = jh - 1;
+            }
+            return;
+        }
+    }
     auto fa = [&](int j) { return fma(double(j), df, f0); };
     auto inside = [&](int j) { return !(fabs((nu - fa(j)) * g) + y >= lim); };
-    const double hq = (lim - y) * q;
     const int jl = find_first(lo, hi, ceil(md - hq), [&](int j) { return fa(j) > nu || inside(j); });
     const int jh = find_first(lo, hi, floor(md + hq) + 1.0, [&](int j) { return fa(j) > nu && !inside(j); });
     if (jl < jh) {
