@@ -153,31 +153,13 @@ __global__ void k_grid_check(GridDev g, unsigned* err) {
 // line; inside, only the lines within the core-candidate reach can have
 // pairs, and step two tests u on them.
 constexpr double kNearR2 = 1.5;
-// Returns the line's core half-width in grid points (Voigt; 0 otherwise).
 // Grid indices [jlo, jhi] of the window [lo, hi) where |x| + y < lim, with
 // x = (nu - f_j) g in FP64 on the analytic grid f_j = f0 + j df: the region
 // choice of the FP64 path (up to the grid's last-bit rounding), so that no
 // pair changes region with the FP32 rounding of x.  Empty: jlo > jhi.
-__device__ void region_interval(double nu, double g, double y, double lim, int lo, int hi, double f0,
-                                double df, int& jlo, int& jhi) {
-    jlo = 1;
-    jhi = 0;
-    if (!(y < lim) || lo >= hi) return;
-    auto fa = [&](int j) { return fma(double(j), df, f0); };
-    auto inside = [&](int j) { return !(fabs((nu - fa(j)) * g) + y >= lim); };
-    const double hw = (lim - y) / g;
-    const int jl = find_first(lo, hi, ceil((nu - hw - f0) / df), [&](int j) { return fa(j) > nu || inside(j); });
-    const int jh = find_first(lo, hi, floor((nu + hw - f0) / df) + 1.0,
-                              [&](int j) { return fa(j) > nu && !inside(j); });
-    if (jl < jh) {
-        jlo = jl;
-        jhi = jh - 1;
-    }
-}
-
-// region_interval with its two starting guesses from precomputed values:
-// md = (nu - f0) / df and q = 1 / (g df) (no division).  The guesses only
-// decide where the walks start; the intervals are the same.
+// md = (nu - f0) / df and q = 1 / (g df) come precomputed; they place the
+// interval's ends, and the region test itself decides where an end is close
+// to a grid point.
 __device__ __forceinline__ void region_interval_q(double nu, double g, double y, double lim, int lo, int hi, double f0,
                                   double df, double md, double q, int& jlo, int& jhi) {
     jlo = 1;
@@ -212,6 +194,12 @@ __device__ __forceinline__ void region_interval_q(double nu, double g, double y,
         jlo = jl;
         jhi = jh - 1;
     }
+}
+
+// region_interval_q with md and q computed here.
+__device__ void region_interval(double nu, double g, double y, double lim, int lo, int hi, double f0,
+                                double df, int& jlo, int& jhi) {
+    region_interval_q(nu, g, y, lim, lo, hi, f0, df, (nu - f0) / df, 1.0 / (g * df), jlo, jhi);
 }
 
 // `reach` (mixed Voigt): the largest distance, in grid points, from the
