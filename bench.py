@@ -488,7 +488,7 @@ def run_ours(args, rank, world, dist):
     f64_value = pairs_step * world / (f64_step * 1e-3) if f64_ms else None
 
     # end-to-end through xs_engine_execute_host: pinned host lines -> device
-    # in 8 slices whose copies overlap step one, sweep, result -> pinned host
+    # in 16 slices whose copies overlap step one, sweep, result -> pinned host
     out_host = torch.empty((nc, npts), dtype=torch.float64).pin_memory()
     h2d = sum(int(host[k].numel() * host[k].element_size()) for k in keys)
     d2h = int(out.numel() * out.element_size())
@@ -500,7 +500,7 @@ def run_ours(args, rank, world, dist):
     s0.record(stream)
     for _ in range(e2e_steps):
         out.zero_()
-        eng.execute_host(o_mix, cc, L_host, L, G, out.data_ptr(), npts, out_host.data_ptr(), pieces=8)
+        eng.execute_host(o_mix, cc, L_host, L, G, out.data_ptr(), npts, out_host.data_ptr(), pieces=16)
     s1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = max_over_ranks(s0.elapsed_time(s1) / e2e_steps) if e2e_steps else float("nan")
