@@ -170,6 +170,40 @@ def test_doppler_cpu_convention_vs_reference_openmp(engine, cuda, threads):
     assert_fp64_parity(got, ref)
 
 
+@pytest.mark.parametrize("profile, convention, threads, pieces",
+                         [(capi.DOPPLER, capi.CONV_GPU, 1, 4), (capi.DOPPLER, capi.CONV_CPU, 3, 7),
+                          (capi.VOIGT, capi.CONV_CPU, 4, 5)])
+def test_execute_host_matches_execute(engine, cuda, profile, convention, threads, pieces):
+    """xs_engine_execute_host (host lines copied in slices that overlap step
+    one) against xs_engine_execute on the same lines already on the device:
+    bit-identical, including the CPU convention's coverage rule (the lines
+    past the threads' blocks are copied but not evaluated)."""
+    import torch
+
+    lines = synth.exomol_like(2003, 3000, seed=6, nu_max=2000.0)
+    grid = synth.Grid(0.0, 2000.0, 200000)
+    cond = dict(temperature=296.0, partition=2844.0, mean_mass=30.01, pressure=1.0)
+    fr = grid.freq()
+    want = run_engine(engine, profile, lines, fr, cond, grid.dfreq, cuda, convention=convention,
+                      cpu_threads=threads)
+    host = {k: v.cpu().pin_memory() for k, v in to_device(lines, cuda).items()}
+    dev = {k: torch.empty_like(v, device=cuda) for k, v in host.items()}
+    dfr = torch.as_tensor(fr, device=cuda)
+    out = torch.zeros((1, len(fr)), dtype=torch.float64, device=cuda)
+    out_host = torch.full((1, len(fr)), -1.0, dtype=torch.float64).pin_memory()
+    opts = capi.make_options(profile, grid.dfreq, cond["mean_mass"], convention=convention,
+                             cpu_threads=threads)
+    cc = [capi.make_condition(cond["temperature"], cond["partition"], 1.0, 1.0, -1.0)]
+    engine.set_stream(torch.cuda.current_stream(cuda).cuda_stream)
+    engine.execute_host(opts, cc, capi.make_lines(host), capi.make_lines(dev), capi.make_grid(dfr),
+                        out.data_ptr(), len(fr), out_host.data_ptr(), pieces=pieces)
+    engine.sync()
+    for k in host:
+        assert torch.equal(dev[k].cpu(), host[k])
+    np.testing.assert_array_equal(out.cpu().numpy()[0], want[0] if want.ndim == 2 else want)
+    np.testing.assert_array_equal(out_host.numpy()[0], want[0] if want.ndim == 2 else want)
+
+
 def test_gaussian_vs_oracle(engine, cuda):
     lines, grid, cond = small_voigt_case(seed=9, n=2000)
     fr = grid.freq()
