@@ -970,7 +970,7 @@ def run_serving(args, dev_index: int):
                      f"{'/'.join(f'{n * args.serve_scale:.0e}' for n, _ in synth.SERVE_MOLECULES)} "
                      "lines (M 18.02/30.01/16.04), T U(200,3000) K, P logU(1e-5,100) bar, "
                      "Doppler/Voigt 1:1, span U(100,5000) cm-1, df logU(0.01,1) cm-1, cut 25; "
-                     f"chunk order {'round robin' if args.serve_policy else 'least remaining work'}")
+                     f"chunk order {['least remaining work', 'round robin', 'earliest deadline'][args.serve_policy]}")
     res["line_evals"] = "window-overlap count (line, point) pairs inside +/-25 cm-1"
     return res
 
@@ -1104,7 +1104,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-policy", type=int, default=0,
-                    help="server chunk order: 0 least remaining work, 1 round robin")
+                    help="server chunk order: 0 least remaining work, 1 round robin, 2 earliest deadline")
     ap.add_argument("--serve-alone", type=int, default=40,
                     help="heaviest requests timed alone for the p99 lower bound")
     ap.add_argument("--serve-scale", type=float, default=1.0,

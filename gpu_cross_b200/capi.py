@@ -15,7 +15,7 @@ from . import build as _build
 XS_OK = 0
 XS_ERR_INVALID, XS_ERR_CUDA, XS_ERR_NOMEM, XS_ERR_UNSORTED, XS_ERR_GRID = 1, 2, 3, 4, 5
 XS_ERR_STATE, XS_ERR_NODEVICE, XS_ERR_TIMEOUT, XS_ERR_UNSUPPORTED = 6, 7, 8, 9
-POLICY_LEAST_WORK, POLICY_ROUND_ROBIN = 0, 1
+POLICY_LEAST_WORK, POLICY_ROUND_ROBIN, POLICY_DEADLINE = 0, 1, 2
 
 GAUSSIAN, DOPPLER, VOIGT, PSUEDO_VOIGT = 0, 1, 2, 3
 CONV_GPU, CONV_CPU = 0, 1

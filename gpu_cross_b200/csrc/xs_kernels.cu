@@ -202,10 +202,11 @@ __device__ void region_interval(double nu, double g, double y, double lim, int l
     region_interval_q(nu, g, y, lim, lo, hi, f0, df, (nu - f0) / df, 1.0 / (g * df), jlo, jhi);
 }
 
-// `reach` (mixed Voigt): the largest distance, in grid points, from the
-// line's nearest grid index to its region interval (the core pass's reach).
-// The mixed-precision multi-condition layout has its own step one
-// (k_prep_group_x); the FP64 one is written here.
+// Step one of one (line, condition).  Returns the line's core half-width in
+// grid points (Voigt; 0 otherwise).  `reach` (mixed Voigt): the largest
+// distance, in grid points, from the line's nearest grid index to its region
+// interval (the core pass's reach).  The mixed-precision multi-condition
+// layout has its own step one (k_prep_lines_x); the FP64 one is written here.
 template <int KIND, int CONV, bool MIXED>
 __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* reach = nullptr) {
     const CondDev& C = a.cond[c];
@@ -1512,9 +1513,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_steptwo_voigt_mc(StepArgs a) {
 // (|x| + y < 15, from step one).
 // ---------------------------------------------------------------------------
 // Resident blocks per SM the mixed multi-condition kernel asks the compiler
-// to fit: 24 warps per SM (about 80 registers a thread), except 8 conditions
-// at 8 warps per block, which keeps 124 registers and 16 warps per SM -- the
-// two occupancy points the autotuner chooses between through the block size.
+// to fit: 24 warps per SM (about 80 registers a thread); 28 at 8 conditions
+// and 4 warps per block (72 registers; 7 blocks of 30.7 KB of staging also
+// fit in shared memory), and 16 at 8 conditions and 8 warps per block (124
+// registers) -- the occupancy points the autotuner chooses between through
+// the block size.
 template <int C, int WARPS>
 constexpr int voigt_mcx_min_blocks() {
     return (C == 8 && WARPS == 8) ? 2 : (C == 8 && WARPS == 4) ? 7 : 24 / WARPS;

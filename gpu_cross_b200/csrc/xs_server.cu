@@ -291,6 +291,11 @@ struct TCache {
     }
 };
 
+// XS_POLICY_DEADLINE: estimated line-evals the device runs per millisecond
+// (a request's deadline is its submission time plus its remaining work at
+// this rate).
+constexpr double kDeadlineRate = 2.0e9;
+
 struct Request {
     unsigned long long id = 0;
     xs_request q{};
@@ -697,13 +702,27 @@ void scheduler(xs_server* s) {
             int total = 0;
             for (const Lane& ln : s->lanes) total += int(ln.flight.size());
             const int cap = int(s->lanes.size());
-            const bool rr = s->cfg.policy == XS_POLICY_ROUND_ROBIN;
+            const int pol = s->cfg.policy;
+            // XS_POLICY_DEADLINE: the request whose deadline -- submission
+            // plus its remaining work at kDeadlineRate -- comes first
+            auto key = [&](const Request* r) {
+                if (pol == XS_POLICY_ROUND_ROBIN) return double(r->last_issue);
+                if (pol == XS_POLICY_DEADLINE)
+                    return std::chrono::duration<double, std::milli>(r->t_submit.time_since_epoch()).count() +
+                           r->remaining / kDeadlineRate;
+                return r->remaining;
+            };
             while (total < cap) {
                 Request* best = nullptr;
+                double best_key = 0.0;
                 for (Request* r : s->active)
-                    if (r->next < r->chunks.size() && int(s->lanes[size_t(r->lane)].flight.size()) < depth &&
-                        (!best || (rr ? r->last_issue < best->last_issue : r->remaining < best->remaining)))
-                        best = r;
+                    if (r->next < r->chunks.size() && int(s->lanes[size_t(r->lane)].flight.size()) < depth) {
+                        const double k = key(r);
+                        if (!best || k < best_key) {
+                            best = r;
+                            best_key = k;
+                        }
+                    }
                 if (!best) break;
                 best->last_issue = ++s->issue_seq;
                 if (!issue(s, best)) {
@@ -766,7 +785,7 @@ int xs_server_create(int device, const xs_server_config* cfg, xs_server** out) {
     if (c.chunk_lines == 0) c.chunk_lines = size_t(1) << 22;
     if (c.host_budget == 0) c.host_budget = size_t(1) << 30;
     if (c.lanes > 16 || c.depth > 8) return sfail(XS_ERR_INVALID, "xs_server_create: lanes <= 16, depth <= 8");
-    if (c.policy != XS_POLICY_LEAST_WORK && c.policy != XS_POLICY_ROUND_ROBIN)
+    if (c.policy != XS_POLICY_LEAST_WORK && c.policy != XS_POLICY_ROUND_ROBIN && c.policy != XS_POLICY_DEADLINE)
         return sfail(XS_ERR_INVALID, "xs_server_create: unknown policy");
     if (c.tcache_bytes == 0) c.tcache_bytes = 4LL << 30;
     auto* s = new xs_server();

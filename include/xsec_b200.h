@@ -390,7 +390,10 @@ typedef struct {
     int policy;           /* which admitted request's chunk goes next:
                              XS_POLICY_LEAST_WORK (0, default): the one with
                              the least remaining work; XS_POLICY_ROUND_ROBIN:
-                             each in turn (processor sharing by chunks) */
+                             each in turn (processor sharing by chunks);
+                             XS_POLICY_DEADLINE: earliest deadline first, a
+                             request's deadline being its submission time
+                             plus its remaining work at 2e9 line-evals/ms */
     long long tcache_bytes; /* device bytes (within device_budget) for the
                              per-temperature intensity caches (0 = 4 GiB;
                              < 0: none).  A cache holds, for one molecule,
@@ -404,6 +407,7 @@ typedef struct {
 } xs_server_config;
 #define XS_POLICY_LEAST_WORK 0
 #define XS_POLICY_ROUND_ROBIN 1
+#define XS_POLICY_DEADLINE 2
 
 typedef struct {
     int molecule;       /* id from xs_server_add_molecule */

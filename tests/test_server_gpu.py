@@ -81,7 +81,7 @@ def random_requests(mid, rng, k):
     return reqs
 
 
-@pytest.mark.parametrize("policy", [capi.POLICY_LEAST_WORK, capi.POLICY_ROUND_ROBIN])
+@pytest.mark.parametrize("policy", [capi.POLICY_LEAST_WORK, capi.POLICY_ROUND_ROBIN, capi.POLICY_DEADLINE])
 def test_same_result_alone_and_in_a_mix(cuda, molecule, policy):
     rng = np.random.default_rng(77)
     srv = capi.Server(0, lanes=4, depth=2, chunk_pairs=5e7, policy=policy)
