@@ -978,8 +978,9 @@ def run_serving(args, dev_index: int):
 def run_extra_configs(args, rank, world, dist) -> dict:
     """The other configurations as extra keys of the default run, each with
     its own timing: "single" (1e7 lines, 7.5e5 points, T 1000 K, P 1 bar;
-    mixed and plain FP64) and "doppler" (the ExoMol-style 1e6-line list,
-    FP64, cut 25 and the reference's 100)."""
+    mixed and plain FP64), "doppler" (the ExoMol-style 1e6-line list, FP64,
+    cut 25 and the reference's 100) and "stream" (5e8 lines generated, those
+    with S >= 1e-30 kept in pinned host memory, 3 timed passes)."""
     import copy
 
     out = {}
@@ -1016,6 +1017,18 @@ def run_extra_configs(args, rank, world, dist) -> dict:
             out["doppler"]["config"] = r["config"]["workload"]
     except Exception as exc:
         out["doppler"] = {"error": f"{type(exc).__name__}: {exc}"}
+    try:
+        a3 = copy.copy(a)
+        a3.workload, a3.lines, a3.steps = "stream", 500_000_000, 3
+        r = run_stream(a3, rank, world, dist)
+        if r is not None:
+            out["stream"] = {k: r.get(k) for k in (
+                "value", "unit", "ms_per_step", "grid_points_per_s", "fp64", "accuracy_vs_fp64", "h2d",
+                "e2e", "gpu_launches")}
+            out["stream"]["config"] = r["config"]["workload"]
+            out["stream"]["lines_kept"] = r["config"]["lines_kept"]
+    except Exception as exc:
+        out["stream"] = {"error": f"{type(exc).__name__}: {exc}"}
     return out
 
 
