@@ -92,11 +92,12 @@ int set_error(int code, const char* msg) { return fail(code, msg); }
 // takes precedence).  Voigt tiles of 32 P points: wide where a line's window
 // spans thousands of points (fewer partial lines per tile, record loads
 // shared by more points), narrow on coarse grids, where a 128-point tile
-// would hold mostly partial and core lines.
+// would hold mostly partial and core lines.  4 warps per block (the mixed
+// kernels then fit 28 warps per SM).
 void default_shape(int kind, bool mixed, double window_points, int* P, int* warps) {
     if (kind == kVoigt) {
         *P = window_points >= 2048.0 ? 4 : (window_points >= 512.0 ? 2 : 1);
-        *warps = mixed ? 8 : 4;
+        *warps = 4;
     } else {
         *P = 1;
         *warps = 8;
