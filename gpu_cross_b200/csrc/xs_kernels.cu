@@ -931,12 +931,13 @@ __device__ __noinline__ int core_queue_flush(WarpCoreQueue<P, MIXED>& cq, int qn
 }
 
 // Resident blocks per SM the step-two Voigt kernel asks the compiler to fit
-// (register budget): 28 warps per SM for the FP32 path at 4 points per thread
-// and 4 warps per block (72 registers; 7 blocks of 24.6 KB of staging fit in
-// shared memory), 24 for its other shapes up to 4 points per thread.
+// (register budget), FP32 path at 4 warps per block: 28 warps per SM at 4
+// points per thread (72 registers), 32 at 1 or 2 (64 registers; 8 blocks of
+// 24.6 KB of staging fit in shared memory); 24 for its other shapes up to 4
+// points per thread.
 template <int P, int WARPS, bool MIXED>
 constexpr int voigt_min_blocks() {
-    return (MIXED && P == 4 && WARPS == 4) ? 7 : (MIXED && P <= 4) ? 24 / WARPS : 1;
+    return (MIXED && P == 4 && WARPS == 4) ? 7 : (MIXED && P <= 2 && WARPS == 4) ? 8 : (MIXED && P <= 4) ? 24 / WARPS : 1;
 }
 
 template <int P, int WARPS, bool MIXED>
