@@ -881,7 +881,8 @@ def run_serving(args, dev_index: int):
     trace = synth.serving_trace(rate=args.serve_rate, duration_s=args.serve_seconds)
     log(f"[serve] {len(mols)} molecules ({sum(len(l) for l, _ in mols):.3e} lines) and "
         f"{len(trace)} requests generated in {time.perf_counter() - t0:.1f} s")
-    srv = capi.Server(dev_index, policy=args.serve_policy)
+    srv = capi.Server(dev_index, policy=args.serve_policy, lanes=args.serve_lanes, depth=args.serve_depth,
+                      chunk_pairs=args.serve_chunk_pairs)
     try:
         mids = [srv.add_molecule(l, m) for l, m in mols]
         del mols
@@ -1118,6 +1119,10 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-policy", type=int, default=0,
                     help="server chunk order: 0 least remaining work, 1 round robin, 2 earliest deadline")
+    ap.add_argument("--serve-lanes", type=int, default=0, help="server streams (0: the server's default)")
+    ap.add_argument("--serve-depth", type=int, default=0, help="chunks in flight per stream (0: default)")
+    ap.add_argument("--serve-chunk-pairs", type=float, default=0.0,
+                    help="target line-evals per served chunk (0: the server's default)")
     ap.add_argument("--serve-alone", type=int, default=40,
                     help="heaviest requests timed alone for the p99 lower bound")
     ap.add_argument("--serve-scale", type=float, default=1.0,
