@@ -178,7 +178,8 @@ __device__ __forceinline__ void region_interval_q(double nu, double g, double y,
         const double bl = md - hq, bh = md + hq;
         const double tol = 1.0e-6 + 1.0e-13 * (fabs(md) + (fabs(nu) + fabs(f0)) / df + hq);
         if (fabs(bl) < 1.0e9 && fabs(bh) < 1.0e9 && fabs(bl - rint(bl)) > tol && fabs(bh - rint(bh)) > tol) {
-            const int jl = clamp_index(ceil(bl), lo, hi), jh = clamp_index(ceil(bh), lo, hi);
+            // ceil to int in one conversion, clamped in integers (lo < hi)
+            const int jl = min(max(__double2int_ru(bl), lo), hi), jh = min(max(__double2int_ru(bh), lo), hi);
             if (jl < jh) {
                 jlo = jl;
                 jhi = jh - 1;
@@ -526,7 +527,8 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
     const double m = rint(md);
     const double nu_df = nu_p / df;  // q = 1 / (g df) = nu_df * dpw
     const bool far_m = !(fabs(m) < 16000000.0);
-    if (live) a.mi[i] = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
+    const int im = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
+    if (live) a.mi[i] = im;
 
     // device_compute_cross_section_voigt_stepone, cross_kernal.cu:775-779
     // (GPU); OpenMPManager.cpp:196-200 (CPU)
@@ -623,9 +625,19 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                 region_interval_q(nu_p, g, y, 15.0, lo, hi, f0, df, md, q, iv.lo15, iv.hi15);
                 region_interval_q(nu_p, g, y, 5.5, lo, hi, f0, df, md, q, iv.lo55, iv.hi55);
                 if (iv.lo15 <= iv.hi15) {
-                    const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
-                    rch = w < 3.0e7 ? int(w) : 30000000;
-                    if (!(w < 3.0e7)) atomicOr(a.err, kErrReach);  // the core pass would not find it
+                    // in integers where m is one (|m| < 1.6e7, grid indices
+                    // below 1.5e7: no overflow)
+                    bool over;
+                    if (far_m) {
+                        const double w = fmax(m - double(iv.lo15), double(iv.hi15) - m);
+                        over = !(w < 3.0e7);
+                        rch = over ? 30000000 : int(w);
+                    } else {
+                        rch = max(im - iv.lo15, iv.hi15 - im);
+                        over = rch >= 30000000;
+                        if (over) rch = 30000000;
+                    }
+                    if (over) atomicOr(a.err, kErrReach);  // the core pass would not find it
                     // |md - j| < sqrt(kNearR2 - y^2) q, |md - m| <= 1/2, one
                     // point of margin, plus one (0: none)
                     // (in FP32, widened by 1e-6 for its rounding)

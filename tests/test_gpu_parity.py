@@ -328,14 +328,26 @@ def test_multi_condition_mixed_edges(engine, cuda, C):
         assert_mixed_parity(mix[k], f64[k])
 
 
-def test_empty_and_outside_lines(engine, cuda):
+@pytest.mark.parametrize("profile,precision,C", [
+    (capi.VOIGT, capi.FP64, 0), (capi.VOIGT, capi.FP64, 2), (capi.VOIGT, capi.MIXED, 1),
+    (capi.VOIGT, capi.MIXED, 8), (capi.DOPPLER, capi.FP64, 0), (capi.GAUSSIAN, capi.FP64, 0)])
+def test_empty_and_outside_lines(engine, cuda, profile, precision, C):
+    """No lines, and lines whose windows miss the grid (beyond it on either
+    side): every kernel path leaves the grid exactly zero."""
     lines, grid, cond = small_voigt_case(seed=2, n=100)
     fr = grid.freq()
-    got = run_engine(engine, capi.VOIGT, lines.slice(0, 0), fr, cond, grid.dfreq, cuda)
-    assert not got.any()
-    far = synth.random_lines(100, 5000.0, 5100.0, 2500.0, 1e-6, 1e2, seed=2)
-    got = run_engine(engine, capi.VOIGT, far, fr, cond, grid.dfreq, cuda)
-    assert not got.any()
+    conds = None
+    if C > 1:
+        conds = [dict(cond, temperature=t, partition=synth.partition_poly(t), gamma_scale=g)
+                 for t in (500.0, 1500.0) for g in ((0.01, 1.0, 10.0, 100.0) if C == 8 else (1.0,))]
+    kw = dict(precision=precision, conds=conds, C=C)
+    got = run_engine(engine, profile, lines.slice(0, 0), fr, cond, grid.dfreq, cuda, **kw)
+    assert not np.asarray(got).any()
+    above = synth.random_lines(100, 5000.0, 5100.0, 2500.0, 1e-6, 1e2, seed=2)
+    below = synth.random_lines(100, 100.0, 200.0, 2500.0, 1e-6, 1e2, seed=3)
+    for far in (above, below):
+        got = run_engine(engine, profile, far, fr, cond, grid.dfreq, cuda, **kw)
+        assert not np.asarray(got).any()
 
 
 def test_unsorted_lines_are_reported(engine, cuda):
