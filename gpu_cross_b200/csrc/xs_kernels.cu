@@ -157,11 +157,15 @@ constexpr double kNearR2 = 1.5;
 // x = (nu - f_j) g in FP64 on the analytic grid f_j = f0 + j df: the region
 // choice of the FP64 path (up to the grid's last-bit rounding), so that no
 // pair changes region with the FP32 rounding of x.  Empty: jlo > jhi.
-// md = (nu - f0) / df and q = 1 / (g df) come precomputed; they place the
-// interval's ends, and the region test itself decides where an end is close
-// to a grid point.
+// md = (nu - f0) / df, q = 1 / (g df) and tb = |md| + (|nu| + |f0|) / df
+// (the line's part of the rounding tolerance below) come precomputed; md and
+// q place the interval's ends, and the region test itself decides where an
+// end is close to a grid point.
+__device__ __forceinline__ double region_tol_base(double nu, double f0, double df, double md) {
+    return fabs(md) + (fabs(nu) + fabs(f0)) / df;
+}
 __device__ __forceinline__ void region_interval_q(double nu, double g, double y, double lim, int lo, int hi, double f0,
-                                  double df, double md, double q, int& jlo, int& jhi) {
+                                  double df, double md, double q, double tb, int& jlo, int& jhi) {
     jlo = 1;
     jhi = 0;
     if (!(y < lim) || lo >= hi) return;
@@ -176,7 +180,7 @@ __device__ __forceinline__ void region_interval_q(double nu, double g, double y,
     // Otherwise the walks below decide.
     {
         const double bl = md - hq, bh = md + hq;
-        const double tol = 1.0e-6 + 1.0e-13 * (fabs(md) + (fabs(nu) + fabs(f0)) / df + hq);
+        const double tol = 1.0e-6 + 1.0e-13 * (tb + hq);
         if (fabs(bl) < 1.0e9 && fabs(bh) < 1.0e9 && fabs(bl - rint(bl)) > tol && fabs(bh - rint(bh)) > tol) {
             // ceil to int in one conversion, clamped in integers (lo < hi)
             const int jl = min(max(__double2int_ru(bl), lo), hi), jh = min(max(__double2int_ru(bh), lo), hi);
@@ -197,10 +201,14 @@ __device__ __forceinline__ void region_interval_q(double nu, double g, double y,
     }
 }
 
-// region_interval_q with md and q computed here.
-__device__ void region_interval(double nu, double g, double y, double lim, int lo, int hi, double f0,
-                                double df, int& jlo, int& jhi) {
-    region_interval_q(nu, g, y, lim, lo, hi, f0, df, (nu - f0) / df, 1.0 / (g * df), jlo, jhi);
+// The intervals of region II-IV (|x| + y < 15) and of regions III-IV
+// (|x| + y < 5.5), with md, q and tb computed once for both.
+__device__ void region_intervals(double nu, double g, double y, int lo, int hi, double f0, double df, int& j15,
+                                 int& k15, int& j55, int& k55) {
+    const double md = (nu - f0) / df, q = 1.0 / (g * df);
+    const double tb = region_tol_base(nu, f0, df, md);
+    region_interval_q(nu, g, y, 15.0, lo, hi, f0, df, md, q, tb, j15, k15);
+    region_interval_q(nu, g, y, 5.5, lo, hi, f0, df, md, q, tb, j55, k55);
 }
 
 // Step one of one (line, condition).  Returns the line's core half-width in
@@ -386,8 +394,7 @@ __device__ __forceinline__ int prep_line(const PrepArgs& a, long i, int c, int* 
             rr.hi = float(hi);
             // exact intervals: step two leaves [clo, chi] to the core pass
             int j15, k15, j55, k55;
-            region_interval(nu_p, g, y, 15.0, lo, hi, f0, df, j15, k15);
-            region_interval(nu_p, g, y, 5.5, lo, hi, f0, df, j55, k55);
+            region_intervals(nu_p, g, y, lo, hi, f0, df, j15, k15, j55, k55);
             int rch = 0;
             if (j15 <= k15) {
                 const double w = fmax(m - double(j15), double(k15) - m);
@@ -526,6 +533,7 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
     const double md = (nu_p - f0) / df;
     const double m = rint(md);
     const double nu_df = nu_p / df;  // q = 1 / (g df) = nu_df * dpw
+    const double tb = region_tol_base(nu_p, f0, df, md);
     const bool far_m = !(fabs(m) < 16000000.0);
     const int im = int(fmin(fmax(m, -1073741824.0), 1073741824.0));
     if (live) a.mi[i] = im;
@@ -622,8 +630,8 @@ __global__ void __launch_bounds__(256, 3) k_prep_lines_x(PrepArgs a) {
                 wide = wide || !(xw * xw + y2 < kPairUMax) || !(fabs(Pc) < kPairPcMax);
                 CoreIv iv;
                 const double q = nu_df * Cd.dpw;
-                region_interval_q(nu_p, g, y, 15.0, lo, hi, f0, df, md, q, iv.lo15, iv.hi15);
-                region_interval_q(nu_p, g, y, 5.5, lo, hi, f0, df, md, q, iv.lo55, iv.hi55);
+                region_interval_q(nu_p, g, y, 15.0, lo, hi, f0, df, md, q, tb, iv.lo15, iv.hi15);
+                region_interval_q(nu_p, g, y, 5.5, lo, hi, f0, df, md, q, tb, iv.lo55, iv.hi55);
                 if (iv.lo15 <= iv.hi15) {
                     // in integers where m is one (|m| < 1.6e7, grid indices
                     // below 1.5e7: no overflow)
