@@ -534,6 +534,10 @@ def run_ours(args, rank, world, dist):
             xu_pct = tj.get("steptwo_mixed_sweep_xu_pipe_pct")
         except (OSError, ValueError):
             traffic = None
+    if args.workload != "sweep" or grid.npoints != 75_000:
+        traffic = xu_pct = None  # measured on the sweep's grid and conditions only
+    elif traffic:
+        traffic = traffic * lines.nu.size / 1e7  # step two's reads grow with the line count
     regions = region_histogram(lines, grid, conds, common) if args.workload == "sweep" else None
 
     # the reference's own GPU kernels (cross_kernal.cu built for sm_100a) on a
